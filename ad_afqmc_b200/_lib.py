@@ -1,0 +1,184 @@
+"""ctypes binding of libafqmc_b200.so (the C ABI in include/afqmc_b200.h).
+
+The library is required: importing the walker-path classes without it, or
+calling them without a CUDA device, raises.  There is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import torch
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libafqmc_b200.so")
+
+AFQ_OK = 0
+AFQ_RESTRICTED, AFQ_UNRESTRICTED = 0, 1
+AFQ_TRIAL_RHF, AFQ_TRIAL_UHF = 0, 1
+AFQ_FP64, AFQ_MIXED = 0, 1
+AFQ_SR_LOCAL, AFQ_SR_GLOBAL = 0, 1
+
+_dp = C.POINTER(C.c_double)
+
+
+class afq_dims(C.Structure):
+    _fields_ = [
+        ("norb", C.c_int32),
+        ("nocc", C.c_int32 * 2),
+        ("nchol", C.c_int32),
+        ("nwalkers", C.c_int32),
+        ("walker_type", C.c_int32),
+        ("trial_type", C.c_int32),
+        ("n_exp_terms", C.c_int32),
+        ("precision", C.c_int32),
+        ("reserved", C.c_int32),
+        ("dt", C.c_double),
+    ]
+
+
+class afq_ham(C.Structure):
+    _fields_ = [
+        ("mo", C.c_void_p * 2),
+        ("rot_h1", C.c_void_p * 2),
+        ("rot_chol", C.c_void_p * 2),
+        ("chol", C.c_void_p),
+        ("exp_h1", C.c_void_p * 2),
+        ("mf_shifts", C.c_void_p),
+        ("h0", C.c_double),
+        ("h0_prop", C.c_double * 2),
+    ]
+
+
+class afq_state(C.Structure):
+    _fields_ = [
+        ("walkers", C.c_void_p * 2),
+        ("weights", C.c_void_p),
+        ("overlaps", C.c_void_p),
+        ("scalars", C.c_void_p),
+    ]
+
+
+class AfqError(RuntimeError):
+    pass
+
+
+_lib: Optional[C.CDLL] = None
+
+_SIGS = {
+    "afq_version": ([], C.c_int),
+    "afq_status_string": ([C.c_int], C.c_char_p),
+    "afq_prepared_size": ([C.POINTER(afq_dims), C.POINTER(C.c_size_t)], C.c_int),
+    "afq_workspace_size": ([C.POINTER(afq_dims), C.POINTER(C.c_size_t)], C.c_int),
+    "afq_small_workspace_size": ([C.POINTER(afq_dims), C.POINTER(C.c_size_t)], C.c_int),
+    "afq_prepare": ([C.POINTER(afq_dims), C.POINTER(afq_ham), C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_calc_overlap": ([C.POINTER(afq_dims), C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_calc_green": ([C.POINTER(afq_dims), C.c_void_p * 2, C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_calc_force_bias": ([C.POINTER(afq_dims), C.c_void_p, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_calc_energy": ([C.POINTER(afq_dims), C.c_void_p, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_propagate_constrained": ([C.POINTER(afq_dims), C.c_void_p, C.POINTER(afq_state), C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_orthonormalize": ([C.POINTER(afq_dims), C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_stochastic_reconfiguration": ([C.POINTER(afq_dims), C.c_void_p, C.c_double, C.c_int, C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "afq_block_end": ([C.POINTER(afq_dims), C.c_void_p, C.POINTER(afq_state), C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_normal_fields": ([C.c_void_p, C.c_int64, C.c_uint64, C.c_uint64, C.c_void_p], C.c_int),
+    "afq_launch_count": ([C.c_int, C.POINTER(C.c_ulonglong)], C.c_int),
+    "afq_profile_begin": ([C.c_int], C.c_int),
+    "afq_profile_end": ([C.POINTER(C.c_double), C.POINTER(C.c_int)], C.c_int),
+}
+
+KERNEL_IDS = {"green": 0, "fb": 1, "prep": 2, "vhs": 3, "prop": 4, "exchange": 5, "ecomb": 6,
+              "weights": 7, "qr": 8, "sr": 9, "gather": 10, "block_end": 11, "normal": 12,
+              "misc": 13}
+
+
+def launch_count(kernel: Optional[str] = None) -> int:
+    c = C.c_ulonglong()
+    kid = -1 if kernel is None else KERNEL_IDS[kernel]
+    check(lib().afq_launch_count(kid, C.byref(c)), "afq_launch_count")
+    return int(c.value)
+
+
+def profile_begin(kernel: str) -> None:
+    check(lib().afq_profile_begin(KERNEL_IDS[kernel]), "afq_profile_begin")
+
+
+def profile_end():
+    ms, n = C.c_double(), C.c_int()
+    check(lib().afq_profile_end(C.byref(ms), C.byref(n)), "afq_profile_end")
+    return float(ms.value), int(n.value)
+
+EXPORTED = tuple(_SIGS)
+
+
+def lib() -> C.CDLL:
+    """Load the library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise AfqError(
+                f"{LIB_PATH} is missing: build it with `python -m ad_afqmc_b200.build` "
+                "(the walker path has no CPU fallback)"
+            )
+        l = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(l, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = l
+    return _lib
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != AFQ_OK:
+        msg = lib().afq_status_string(rc).decode()
+        raise AfqError(f"{what}: {msg} (status {rc})")
+
+
+def require_cuda(t: torch.Tensor, name: str = "tensor") -> None:
+    if not t.is_cuda:
+        raise AfqError(f"{name} must be a CUDA tensor (the walker path has no CPU fallback)")
+    if not t.is_contiguous():
+        raise AfqError(f"{name} must be contiguous")
+
+
+def ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def pair(a, b=None):
+    arr = (C.c_void_p * 2)()
+    arr[0] = a
+    arr[1] = b
+    return arr
+
+
+def stream_handle(stream: Optional[torch.cuda.Stream] = None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def make_dims(norb, nocc, nchol, nwalkers, walker_type, trial_type, n_exp_terms, precision, dt):
+    d = afq_dims()
+    d.norb = int(norb)
+    d.nocc[0] = int(nocc[0])
+    d.nocc[1] = int(nocc[1])
+    d.nchol = int(nchol)
+    d.nwalkers = int(nwalkers)
+    d.walker_type = int(walker_type)
+    d.trial_type = int(trial_type)
+    d.n_exp_terms = int(n_exp_terms)
+    d.precision = int(precision)
+    d.reserved = 0
+    d.dt = float(dt)
+    return d
+
+
+def sizes(d: afq_dims):
+    p, w = C.c_size_t(), C.c_size_t()
+    check(lib().afq_prepared_size(C.byref(d), C.byref(p)), "afq_prepared_size")
+    check(lib().afq_workspace_size(C.byref(d), C.byref(w)), "afq_workspace_size")
+    return p.value, w.value

@@ -1,0 +1,337 @@
+// extern "C" entry points of libafqmc_b200.so (declared in include/afqmc_b200.h).
+#include <cuda_runtime.h>
+
+#include "afqmc_b200.h"
+#include "layout.cuh"
+#include "ops.h"
+
+using namespace afq;
+
+namespace {
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+#define AFQ_TRY(expr)                          \
+  do {                                         \
+    cudaError_t _e = (expr);                   \
+    if (_e != cudaSuccess) return AFQ_ERR_CUDA; \
+  } while (0)
+
+int check_common(const afq_dims* d, Layout& L, const void* prepared, void* work,
+                 size_t work_bytes) {
+  int rc = make_layout(d, L);
+  if (rc != AFQ_OK) return rc;
+  if (!prepared || !work) return AFQ_ERR_NULL;
+  if (!aligned16(prepared) || !aligned16(work)) return AFQ_ERR_ALIGN;
+  if (work_bytes < (size_t)L.work * sizeof(double)) return AFQ_ERR_WORKSPACE;
+  return AFQ_OK;
+}
+
+int check_walkers(const Layout& L, const double* const w[2]) {
+  if (!w || !w[0]) return AFQ_ERR_NULL;
+  if (!aligned16(w[0])) return AFQ_ERR_ALIGN;
+  if (L.ns == 2) {
+    if (!w[1]) return AFQ_ERR_NULL;
+    if (!aligned16(w[1])) return AFQ_ERR_ALIGN;
+  }
+  return AFQ_OK;
+}
+
+GreenArgs green_args_mo(const Layout& L, const double* const mo[2], double* work,
+                        const double* const walkers[2]) {
+  GreenArgs a{};
+  a.N = L.N;
+  a.W = L.W;
+  a.ns = L.ns;
+  a.wscal = work + L.w_wscal;
+  a.gpl = nullptr;
+  a.ldg = L.Kfb;
+  for (int s = 0; s < L.ns; ++s) {
+    a.sec[s].walk = walkers[s];
+    a.sec[s].mo = mo[L.uhf_trial ? s : 0];
+    a.sec[s].rh1 = nullptr;
+    a.sec[s].no = L.no[s];
+    a.sec[s].koff = L.koff[s];
+    a.sec[s].theta = nullptr;
+    a.sec[s].gout = nullptr;
+  }
+  return a;
+}
+
+GreenArgs green_args(const Layout& L, const double* prep, double* work,
+                     const double* const walkers[2]) {
+  const double* mo[2] = {prep + L.p_mo[0], prep + L.p_mo[1]};
+  return green_args_mo(L, mo, work, walkers);
+}
+
+int check_small(const afq_dims* d, Layout& L, void* work, size_t work_bytes) {
+  int rc = make_layout(d, L);
+  if (rc != AFQ_OK) return rc;
+  if (!work) return AFQ_ERR_NULL;
+  if (!aligned16(work)) return AFQ_ERR_ALIGN;
+  if (work_bytes < (size_t)L.W * 16 * sizeof(double)) return AFQ_ERR_WORKSPACE;
+  return AFQ_OK;
+}
+
+// energy of the current walkers into wscal[.,14..15] and optionally eout
+int energy_impl(const Layout& L, const double* prep, double* work, const double* const walkers[2],
+                double* eout, int eout_stride, cudaStream_t st) {
+  GreenArgs a = green_args(L, prep, work, walkers);
+  for (int s = 0; s < L.ns; ++s) {
+    a.sec[s].theta = work + L.w_theta[s];
+    a.sec[s].rh1 = prep + L.p_rh1[s];
+  }
+  AFQ_TRY(launch_green(a, st));
+  for (int s = 0; s < L.ns; ++s) AFQ_TRY(launch_exchange(L, prep, work, s, st));
+  AFQ_TRY(launch_energy_combine(L, prep, work, eout, eout_stride, st));
+  return AFQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int afq_version(void) { return 100; }
+
+const char* afq_status_string(int status) {
+  switch (status) {
+    case AFQ_OK: return "ok";
+    case AFQ_ERR_SHAPE: return "unsupported or inconsistent sizes";
+    case AFQ_ERR_NULL: return "a required pointer is NULL";
+    case AFQ_ERR_CUDA: return "CUDA runtime error";
+    case AFQ_ERR_WORKSPACE: return "prepared/workspace buffer too small";
+    case AFQ_ERR_ALIGN: return "pointer not 16-byte aligned";
+    case AFQ_ERR_ARG: return "argument out of range";
+    default: return "unknown status";
+  }
+}
+
+int afq_prepared_size(const afq_dims* d, size_t* bytes) {
+  Layout L;
+  int rc = make_layout(d, L);
+  if (rc != AFQ_OK) return rc;
+  if (!bytes) return AFQ_ERR_NULL;
+  *bytes = (size_t)L.prepared * sizeof(double);
+  return AFQ_OK;
+}
+
+int afq_workspace_size(const afq_dims* d, size_t* bytes) {
+  Layout L;
+  int rc = make_layout(d, L);
+  if (rc != AFQ_OK) return rc;
+  if (!bytes) return AFQ_ERR_NULL;
+  *bytes = (size_t)L.work * sizeof(double);
+  return AFQ_OK;
+}
+
+int afq_prepare(const afq_dims* d, const afq_ham* h, void* prepared, size_t prepared_bytes,
+                void* stream) {
+  Layout L;
+  int rc = make_layout(d, L);
+  if (rc != AFQ_OK) return rc;
+  if (!h || !prepared) return AFQ_ERR_NULL;
+  if (!aligned16(prepared)) return AFQ_ERR_ALIGN;
+  if (prepared_bytes < (size_t)L.prepared * sizeof(double)) return AFQ_ERR_WORKSPACE;
+  const int ntr = L.uhf_trial ? 2 : 1;
+  for (int s = 0; s < ntr; ++s)
+    if (!h->mo[s] || !h->rot_h1[s] || !h->rot_chol[s]) return AFQ_ERR_NULL;
+  if (!h->chol) return AFQ_ERR_NULL;
+  cudaStream_t st = as_stream(stream);
+  double* P = static_cast<double*>(prepared);
+  const size_t D = sizeof(double);
+  AFQ_TRY(cudaMemsetAsync(P, 0, (size_t)L.prepared * D, st));
+  const int N = L.N;
+  for (int s = 0; s < ntr; ++s) {
+    const int no = L.no[s];
+    AFQ_TRY(cudaMemcpyAsync(P + L.p_mo[s], h->mo[s], (size_t)N * no * D, cudaMemcpyDeviceToDevice,
+                            st));
+    AFQ_TRY(cudaMemcpyAsync(P + L.p_rh1[s], h->rot_h1[s], (size_t)no * N * D,
+                            cudaMemcpyDeviceToDevice, st));
+    AFQ_TRY(cudaMemcpy2DAsync(P + L.p_rc[s], (size_t)L.Npad * D, h->rot_chol[s], (size_t)N * D,
+                              (size_t)N * D, (size_t)L.G * no, cudaMemcpyDeviceToDevice, st));
+  }
+  for (int s = 0; s < L.ns; ++s) {
+    const int ts = L.uhf_trial ? s : 0;
+    const size_t row = (size_t)L.no[s] * N * D;
+    AFQ_TRY(cudaMemcpy2DAsync(P + L.p_rccat + L.koff[s], (size_t)L.Kfb * D, h->rot_chol[ts], row,
+                              row, (size_t)L.G, cudaMemcpyDeviceToDevice, st));
+  }
+  AFQ_TRY(cudaMemcpy2DAsync(P + L.p_chol, (size_t)L.N2pad * D, h->chol, (size_t)N * N * D,
+                            (size_t)N * N * D, (size_t)L.G, cudaMemcpyDeviceToDevice, st));
+  for (int s = 0; s < L.np; ++s)
+    if (h->exp_h1[s])
+      AFQ_TRY(cudaMemcpy2DAsync(P + L.p_exph1[s], (size_t)L.Npad * D, h->exp_h1[s], (size_t)N * D,
+                              (size_t)N * D, (size_t)N, cudaMemcpyDeviceToDevice, st));
+  if (h->mf_shifts)
+    AFQ_TRY(cudaMemcpyAsync(P + L.p_mf, h->mf_shifts, (size_t)L.G * 2 * D, cudaMemcpyDeviceToDevice,
+                          st));
+  AFQ_TRY(launch_set_scalars(P + L.p_scal, h->h0, h->h0_prop[0], h->h0_prop[1], 0.0, st));
+  return AFQ_OK;
+}
+
+int afq_small_workspace_size(const afq_dims* d, size_t* bytes) {
+  Layout L;
+  int rc = make_layout(d, L);
+  if (rc != AFQ_OK) return rc;
+  if (!bytes) return AFQ_ERR_NULL;
+  *bytes = (size_t)L.W * 16 * sizeof(double);
+  return AFQ_OK;
+}
+
+int afq_calc_overlap(const afq_dims* d, const double* const mo[2], const double* const walkers[2],
+                     double* overlaps, void* work, size_t work_bytes, void* stream) {
+  Layout L;
+  int rc = check_small(d, L, work, work_bytes);
+  if (rc != AFQ_OK) return rc;
+  if ((rc = check_walkers(L, walkers)) != AFQ_OK) return rc;
+  if (!overlaps || !mo || !mo[0] || (L.uhf_trial && !mo[1])) return AFQ_ERR_NULL;
+  double* Wk = static_cast<double*>(work);
+  cudaStream_t st = as_stream(stream);
+  GreenArgs a = green_args_mo(L, mo, Wk, walkers);
+  a.wscal = Wk;
+  AFQ_TRY(launch_green(a, st));
+  AFQ_TRY(launch_ovlp_combine(L.W, L.ns, L.mult, Wk, overlaps, 2, st));
+  return AFQ_OK;
+}
+
+int afq_calc_green(const afq_dims* d, const double* const mo[2], const double* const walkers[2],
+                   double* const green[2], void* work, size_t work_bytes, void* stream) {
+  Layout L;
+  int rc = check_small(d, L, work, work_bytes);
+  if (rc != AFQ_OK) return rc;
+  if ((rc = check_walkers(L, walkers)) != AFQ_OK) return rc;
+  if (!green || !green[0] || (L.ns == 2 && !green[1])) return AFQ_ERR_NULL;
+  if (!mo || !mo[0] || (L.uhf_trial && !mo[1])) return AFQ_ERR_NULL;
+  double* Wk = static_cast<double*>(work);
+  GreenArgs a = green_args_mo(L, mo, Wk, walkers);
+  a.wscal = Wk;
+  for (int s = 0; s < L.ns; ++s) a.sec[s].gout = green[s];
+  AFQ_TRY(launch_green(a, as_stream(stream)));
+  return AFQ_OK;
+}
+
+int afq_calc_force_bias(const afq_dims* d, const void* prepared, const double* const walkers[2],
+                        double* force_bias, void* work, size_t work_bytes, void* stream) {
+  Layout L;
+  int rc = check_common(d, L, prepared, work, work_bytes);
+  if (rc != AFQ_OK) return rc;
+  if ((rc = check_walkers(L, walkers)) != AFQ_OK) return rc;
+  if (!force_bias) return AFQ_ERR_NULL;
+  const double* P = static_cast<const double*>(prepared);
+  double* Wk = static_cast<double*>(work);
+  cudaStream_t st = as_stream(stream);
+  GreenArgs a = green_args(L, P, Wk, walkers);
+  a.gpl = Wk + L.w_gpl;
+  AFQ_TRY(launch_green(a, st));
+  AFQ_TRY(launch_fb_gemm(L, P, Wk, st));
+  AFQ_TRY(launch_prep(L, P, Wk, nullptr, d->dt, force_bias, st));
+  return AFQ_OK;
+}
+
+int afq_calc_energy(const afq_dims* d, const void* prepared, const double* const walkers[2],
+                    double* energies, void* work, size_t work_bytes, void* stream) {
+  Layout L;
+  int rc = check_common(d, L, prepared, work, work_bytes);
+  if (rc != AFQ_OK) return rc;
+  if ((rc = check_walkers(L, walkers)) != AFQ_OK) return rc;
+  if (!energies) return AFQ_ERR_NULL;
+  return energy_impl(L, static_cast<const double*>(prepared), static_cast<double*>(work), walkers,
+                     energies, 2, as_stream(stream));
+}
+
+int afq_propagate_constrained(const afq_dims* d, const void* prepared, afq_state* s,
+                              const double* fields, void* work, size_t work_bytes,
+                              void* stream) {
+  Layout L;
+  int rc = check_common(d, L, prepared, work, work_bytes);
+  if (rc != AFQ_OK) return rc;
+  if (!s || !fields || !s->weights || !s->overlaps || !s->scalars) return AFQ_ERR_NULL;
+  const double* const wc[2] = {s->walkers[0], s->walkers[1]};
+  if ((rc = check_walkers(L, wc)) != AFQ_OK) return rc;
+  const double* P = static_cast<const double*>(prepared);
+  double* Wk = static_cast<double*>(work);
+  cudaStream_t st = as_stream(stream);
+  // force bias of the current walkers
+  GreenArgs a = green_args(L, P, Wk, wc);
+  a.gpl = Wk + L.w_gpl;
+  AFQ_TRY(launch_green(a, st));
+  AFQ_TRY(launch_fb_gemm(L, P, Wk, st));
+  AFQ_TRY(launch_prep(L, P, Wk, fields, d->dt, nullptr, st));
+  // VHS and the Trotterized propagator
+  AFQ_TRY(launch_vhs_gemm(L, P, Wk, st));
+  AFQ_TRY(launch_propagate_walkers(L, P, Wk, s->walkers, d->n_exp_terms, st));
+  // new overlaps and the phaseless weight update
+  GreenArgs b = green_args(L, P, Wk, wc);
+  AFQ_TRY(launch_green(b, st));
+  AFQ_TRY(launch_ovlp_combine(L.W, L.ns, L.mult, Wk + L.w_wscal, Wk + L.w_wscal + 12, 16, st));
+  AFQ_TRY(launch_weight_update(L, P, Wk, s->weights, s->overlaps, s->scalars, d->dt, st));
+  return AFQ_OK;
+}
+
+int afq_orthonormalize(const afq_dims* d, double* const walkers[2], double* norms, void* work,
+                       size_t work_bytes, void* stream) {
+  Layout L;
+  int rc = make_layout(d, L);
+  if (rc != AFQ_OK) return rc;
+  if (!work) return AFQ_ERR_NULL;
+  if (!aligned16(work)) return AFQ_ERR_ALIGN;
+  if (work_bytes < (size_t)L.W * 16 * sizeof(double)) return AFQ_ERR_WORKSPACE;
+  const double* const wc[2] = {walkers ? walkers[0] : nullptr, walkers ? walkers[1] : nullptr};
+  if ((rc = check_walkers(L, wc)) != AFQ_OK) return rc;
+  AFQ_TRY(launch_qr(L, walkers, norms, static_cast<double*>(work), as_stream(stream)));
+  return AFQ_OK;
+}
+
+int afq_stochastic_reconfiguration(const afq_dims* d, const double* weights_in, double zeta,
+                                   int mode, const double* const walkers_in[2],
+                                   double* const walkers_out[2], double* weights_out,
+                                   int32_t* indices, void* stream) {
+  Layout L;
+  int rc = make_layout(d, L);
+  if (rc != AFQ_OK) return rc;
+  if (mode != AFQ_SR_LOCAL && mode != AFQ_SR_GLOBAL) return AFQ_ERR_ARG;
+  if (!weights_in || !weights_out || !indices) return AFQ_ERR_NULL;
+  if (L.W > kMaxSrWalkers) return AFQ_ERR_SHAPE;
+  if (weights_out == weights_in) return AFQ_ERR_ARG;
+  cudaStream_t st = as_stream(stream);
+  AFQ_TRY(launch_sr(L.W, weights_in, zeta, mode, weights_out, indices, st));
+  if (walkers_in && walkers_out) {
+    for (int s = 0; s < L.ns; ++s) {
+      if (!walkers_in[s] || !walkers_out[s]) return AFQ_ERR_NULL;
+      if (walkers_in[s] == walkers_out[s]) return AFQ_ERR_ARG;
+      AFQ_TRY(launch_gather(L.W, (long long)L.N * 2 * L.no[s], walkers_in[s], walkers_out[s],
+                            indices, st));
+    }
+  }
+  return AFQ_OK;
+}
+
+int afq_block_end(const afq_dims* d, const void* prepared, afq_state* s, double* block_out,
+                  void* work, size_t work_bytes, void* stream) {
+  Layout L;
+  int rc = check_common(d, L, prepared, work, work_bytes);
+  if (rc != AFQ_OK) return rc;
+  if (!s || !s->weights || !s->overlaps || !s->scalars || !block_out) return AFQ_ERR_NULL;
+  const double* const wc[2] = {s->walkers[0], s->walkers[1]};
+  if ((rc = check_walkers(L, wc)) != AFQ_OK) return rc;
+  const double* P = static_cast<const double*>(prepared);
+  double* Wk = static_cast<double*>(work);
+  cudaStream_t st = as_stream(stream);
+  AFQ_TRY(launch_qr(L, s->walkers, nullptr, Wk, st));
+  rc = energy_impl(L, P, Wk, wc, Wk + L.w_wscal + 14, 16, st);
+  if (rc != AFQ_OK) return rc;
+  AFQ_TRY(launch_ovlp_combine(L.W, L.ns, L.mult, Wk + L.w_wscal, s->overlaps, 2, st));
+  AFQ_TRY(launch_block_end(L, Wk, s->weights, s->scalars, d->dt, block_out, st));
+  return AFQ_OK;
+}
+
+int afq_normal_fields(double* out, int64_t n, uint64_t seed, uint64_t offset, void* stream) {
+  if (!out) return AFQ_ERR_NULL;
+  if (n < 0) return AFQ_ERR_ARG;
+  if (n == 0) return AFQ_OK;
+  AFQ_TRY(launch_normal(out, n, seed, offset, as_stream(stream)));
+  return AFQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,156 @@
+// Device-memory layout of the prepared Hamiltonian and of the workspace.
+//
+// All leading dimensions are padded to an even number of doubles so that
+// every row starts on a 16-byte boundary (cp.async / vector loads).
+#pragma once
+
+#include <stddef.h>
+
+#include "afqmc_b200.h"
+
+namespace afq {
+
+constexpr int kMaxOcc = 60;  // largest occupied block per spin accepted by the kernels
+
+inline long long round_even(long long x) { return (x + 1) & ~1LL; }
+inline long long align_up(long long x, long long a) { return (x + a - 1) / a * a; }
+
+// Exchange-energy tile choice (see exchange kernel): gpt Cholesky vectors
+// per 120-row tile and wpt walkers per BN-column tile.
+struct ExchTile {
+  int bn;   // 80 or 120
+  int gpt;  // Cholesky vectors per tile
+  int wpt;  // walkers per tile
+  int mt;   // number of row tiles = ceil(G / gpt)
+};
+
+struct Layout {
+  // sizes
+  int N, G, W, no[2], ns, np, mult, restricted, uhf_trial, nomax;
+  long long Npad, N2pad, Gpad, Kfb, Kfb_used, koff[2];
+  int splitk;
+  ExchTile ex[2];
+  // prepared buffer offsets (doubles)
+  long long p_mo[2], p_rh1[2], p_rc[2], p_rccat, p_chol, p_exph1[2], p_mf, p_scal, prepared;
+  // workspace offsets (doubles)
+  long long w_gpl, w_theta[2], w_fbpart, w_xt, w_wscal, w_vhs, w_y, w_acc, w_ta, w_tb;
+  long long w_c[2], w_exc[2], w_cum, w_idx, w_misc, work;
+};
+
+inline ExchTile choose_exch_tile(int no, int G, int W) {
+  ExchTile best{80, 1, 1, G};
+  double best_eff = -1.0;
+  const int bns[2] = {80, 120};
+  for (int i = 0; i < 2; ++i) {
+    const int bn = bns[i];
+    if (2 * no > bn || no > 120) continue;
+    const int gpt = 120 / no, wpt = bn / (2 * no);
+    const double eff = double(gpt * no) / 120.0 * double(wpt * 2 * no) / double(bn);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = ExchTile{bn, gpt, wpt, (G + gpt - 1) / gpt};
+    }
+  }
+  return best;
+}
+
+// Returns AFQ_OK and fills L, or a shape error.
+inline int make_layout(const afq_dims* d, Layout& L) {
+  if (!d) return AFQ_ERR_NULL;
+  if (d->norb <= 0 || d->nchol <= 0 || d->nwalkers <= 0) return AFQ_ERR_SHAPE;
+  if (d->walker_type != AFQ_RESTRICTED && d->walker_type != AFQ_UNRESTRICTED) return AFQ_ERR_ARG;
+  if (d->trial_type != AFQ_TRIAL_RHF && d->trial_type != AFQ_TRIAL_UHF) return AFQ_ERR_ARG;
+  if (d->precision != AFQ_FP64 && d->precision != AFQ_MIXED) return AFQ_ERR_ARG;
+  if (d->n_exp_terms < 1 || d->n_exp_terms > 32) return AFQ_ERR_ARG;
+  L.N = d->norb;
+  L.G = d->nchol;
+  L.W = d->nwalkers;
+  L.restricted = d->walker_type == AFQ_RESTRICTED;
+  L.uhf_trial = d->trial_type == AFQ_TRIAL_UHF;
+  if (L.restricted && L.uhf_trial) return AFQ_ERR_SHAPE;  // uhf trial needs unrestricted walkers
+  L.no[0] = d->nocc[0];
+  L.no[1] = L.restricted ? d->nocc[0] : d->nocc[1];
+  if (!L.uhf_trial && L.no[0] != L.no[1]) return AFQ_ERR_SHAPE;  // rhf requires Na == Nb
+  L.ns = L.restricted ? 1 : 2;
+  L.np = L.ns;
+  L.mult = L.restricted ? 2 : 1;
+  // the exchange tile holds one walker's 2*No columns in at most 120
+  for (int s = 0; s < L.ns; ++s)
+    if (L.no[s] <= 0 || L.no[s] > kMaxOcc || L.no[s] > L.N) return AFQ_ERR_SHAPE;
+  if (L.W > (1 << 16)) return AFQ_ERR_SHAPE;
+  L.nomax = L.no[0] > L.no[1] ? L.no[0] : L.no[1];
+  L.Npad = round_even(L.N);
+  L.N2pad = round_even((long long)L.N * L.N);
+  L.Gpad = round_even(L.G);
+  L.koff[0] = 0;
+  L.koff[1] = (long long)L.no[0] * L.N;
+  long long kfb = 0;
+  for (int s = 0; s < L.ns; ++s) kfb += (long long)L.no[s] * L.N;
+  L.Kfb_used = kfb;  // columns actually written; the padding is never read
+  L.Kfb = round_even(kfb);
+  // split-K for the force-bias GEMM so that the grid covers the SMs twice
+  {
+    const long long tiles = ((2LL * L.W + 127) / 128) * ((L.G + 127) / 128);
+    int sk = 1;
+    while (tiles * sk < 296 && sk < 8 && L.Kfb / (sk * 2) >= 256) sk *= 2;
+    L.splitk = sk;
+  }
+  for (int s = 0; s < 2; ++s) L.ex[s] = choose_exch_tile(L.no[s], L.G, L.W);
+
+  // ---- prepared buffer
+  long long o = 0;
+  auto take = [&](long long n) {
+    long long r = o;
+    o += align_up(n, 32);  // 256-byte aligned sub-buffers
+    return r;
+  };
+  const int ntr = L.uhf_trial ? 2 : 1;
+  for (int s = 0; s < 2; ++s) {
+    L.p_mo[s] = L.p_rh1[s] = L.p_rc[s] = -1;
+    L.p_exph1[s] = -1;
+  }
+  for (int s = 0; s < ntr; ++s) {
+    L.p_mo[s] = take((long long)L.N * L.no[s]);
+    L.p_rh1[s] = take((long long)L.no[s] * L.N);
+    L.p_rc[s] = take((long long)L.G * L.no[s] * L.Npad);
+  }
+  if (!L.uhf_trial) {
+    L.p_mo[1] = L.p_mo[0];
+    L.p_rh1[1] = L.p_rh1[0];
+    L.p_rc[1] = L.p_rc[0];
+  }
+  L.p_rccat = take((long long)L.G * L.Kfb);
+  L.p_chol = take((long long)L.G * L.N2pad);
+  for (int s = 0; s < L.np; ++s) L.p_exph1[s] = take((long long)L.N * L.Npad);
+  L.p_mf = take(2LL * L.G);
+  L.p_scal = take(8);
+  L.prepared = o;
+
+  // ---- workspace
+  o = 0;
+  const long long W = L.W, N = L.N;
+  L.w_gpl = take(W * 2 * L.Kfb);
+  for (int s = 0; s < 2; ++s) L.w_theta[s] = -1;
+  for (int s = 0; s < L.ns; ++s) L.w_theta[s] = take(W * N * 2 * L.no[s]);
+  L.w_fbpart = take((long long)L.splitk * 2 * W * L.Gpad);
+  L.w_xt = take(2 * W * L.Gpad);
+  L.w_wscal = take(W * 16);
+  L.w_vhs = take(W * N * 2 * L.Npad);
+  const long long pb = W * N * 2 * L.nomax;
+  L.w_y = take(pb);
+  L.w_acc = take(pb);
+  L.w_ta = take(pb);
+  L.w_tb = take(pb);
+  for (int s = 0; s < 2; ++s) L.w_c[s] = L.w_exc[s] = -1;
+  for (int s = 0; s < L.ns; ++s) {
+    L.w_c[s] = take(W * L.G * 2);
+    L.w_exc[s] = take((long long)L.ex[s].mt * W * 2);
+  }
+  L.w_cum = take(W);
+  L.w_idx = take(W);  // int32 indices stored in double slots
+  L.w_misc = take(64);
+  L.work = o;
+  return AFQ_OK;
+}
+
+}  // namespace afq

@@ -1,0 +1,431 @@
+// Per-walker scalar and walker-matrix operations of the phaseless path:
+//   phaseless weight update      propagation.py:302-335
+//   Householder QR (orthonormalize)  linalg_utils.py:51-72 (LAPACK zgeqr2/zung2r)
+//   comb reconfiguration         sr.py:24-48 (local), sr.py:52-153 (global, 1 rank)
+//   block-end energy statistics  sampling.py:76-94
+//   Gaussian auxiliary fields    Philox4x32-10 + Box-Muller (counter based)
+#include "common.cuh"
+#include "ops.h"
+#include "profile.cuh"
+
+namespace afq {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// weight update (single CTA: needs the total weight for the population shift)
+// ---------------------------------------------------------------------------
+constexpr int kWeightThreads = 1024;
+
+__global__ void __launch_bounds__(kWeightThreads)
+    weight_kernel(int W, double dt, const double* scal, const double* wscal, double* weights,
+                  double* overlaps, double* scalars) {
+  __shared__ double red[kWeightThreads / 32];
+  const double sdt = sqrt(dt);
+  const double h0r = scal[1], h0i = scal[2];
+  const double est = scalars[0], pop = scalars[1];
+  double tot = 0.0;
+  for (int w = threadIdx.x; w < W; w += blockDim.x) {
+    const double* s = wscal + (long long)w * 16;
+    const double2 on = make_double2(s[12], s[13]);
+    const double2 oo = make_double2(overlaps[2 * w], overlaps[2 * w + 1]);
+    const double2 ratio = cdiv(on, oo);
+    // imp = exp(-sqrt(dt) shift + fb_term + dt (pop + h0_prop)) * ratio
+    const double ar = -sdt * s[0] + s[2] + dt * (pop + h0r);
+    const double ai = -sdt * s[1] + s[3] + dt * h0i;
+    const double ea = exp(ar);
+    double sn, cs;
+    sincos(ai, &sn, &cs);
+    const double2 imp = cmul(make_double2(ea * cs, ea * sn), ratio);
+    // theta = angle(exp(-sqrt(dt) shift) * ratio)
+    const double eb = exp(-sdt * s[0]);
+    double sb, cb;
+    sincos(-sdt * s[1], &sb, &cb);
+    const double2 z = cmul(make_double2(eb * cb, eb * sb), ratio);
+    const double th = atan2(z.y, z.x);
+    double ipl = hypot(imp.x, imp.y) * cos(th);
+    if (isnan(ipl)) ipl = 0.0;
+    if (ipl < 1.0e-3) ipl = 0.0;
+    if (ipl > 100.0) ipl = 0.0;
+    double wn = ipl * weights[w];
+    if (wn > 100.0) wn = 0.0;
+    weights[w] = wn;
+    overlaps[2 * w] = on.x;
+    overlaps[2 * w + 1] = on.y;
+    tot += wn;
+  }
+  tot = block_sum(tot, red);
+  if (threadIdx.x == 0) scalars[1] = est - 0.1 * log(tot / W) / dt;
+}
+
+// ---------------------------------------------------------------------------
+// Householder QR, LAPACK convention (zlarfg: beta = -sign(Re a) |x|,
+// tau = ((beta - ar)/beta, -ai/beta), v = x / (a - beta)), explicit Q as zung2r.
+// A is a generic pointer (shared or global memory), row stride lda (double2).
+// ---------------------------------------------------------------------------
+constexpr int kQrThreads = 256;
+
+__device__ void qr_inplace(double2* A, int lda, int N, int no, double2* tau, double* beta,
+                           double2* wv, double2* wpart, double* red, double2* scal_s) {
+  const int tid = threadIdx.x;
+  constexpr int T = kQrThreads;
+  for (int k = 0; k < no; ++k) {
+    double s = 0.0;
+    for (int p = k + 1 + tid; p < N; p += T) {
+      const double2 v = A[p * lda + k];
+      s += v.x * v.x + v.y * v.y;
+    }
+    s = block_sum(s, red);
+    if (tid == 0) {
+      const double2 al = A[k * lda + k];
+      if (s == 0.0 && al.y == 0.0) {
+        tau[k] = make_double2(0.0, 0.0);
+        beta[k] = al.x;
+        *scal_s = make_double2(1.0, 0.0);
+      } else {
+        const double b = -copysign(sqrt(al.x * al.x + al.y * al.y + s), al.x);
+        tau[k] = make_double2((b - al.x) / b, -al.y / b);
+        beta[k] = b;
+        *scal_s = cdiv(make_double2(1.0, 0.0), make_double2(al.x - b, al.y));
+      }
+    }
+    __syncthreads();
+    const double2 sc = *scal_s;
+    const double2 tk = tau[k];
+    for (int p = k + 1 + tid; p < N; p += T) A[p * lda + k] = cmul(A[p * lda + k], sc);
+    if (tid == 0) A[k * lda + k] = make_double2(1.0, 0.0);
+    __syncthreads();
+    const int nj = no - k - 1;
+    if (nj > 0 && (tk.x != 0.0 || tk.y != 0.0)) {
+      // w_j = sum_p conj(v_p) A[p][j]
+      const int nrs = T / nj;
+      if (tid < nrs * nj) {
+        const int j = k + 1 + tid % nj, rs = tid / nj;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int p = k + rs; p < N; p += nrs) acc = cadd(acc, cmul(cconj(A[p * lda + k]), A[p * lda + j]));
+        wpart[tid] = acc;
+      }
+      __syncthreads();
+      for (int j = tid; j < nj; j += T) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int rs = 0; rs < nrs; ++rs) acc = cadd(acc, wpart[rs * nj + j]);
+        wv[j] = acc;
+      }
+      __syncthreads();
+      // A[p][j] -= conj(tau) v_p w_j     (H^H applied from the left)
+      const double2 ct = cconj(tk);
+      const int rows = N - k;
+      for (int e = tid; e < rows * nj; e += T) {
+        const int p = k + e / nj, j = e - (e / nj) * nj;
+        const double2 vp = A[p * lda + k];
+        A[p * lda + k + 1 + j] = csub(A[p * lda + k + 1 + j], cmul(ct, cmul(vp, wv[j])));
+      }
+      __syncthreads();
+    }
+    if (tid == 0) A[k * lda + k] = make_double2(beta[k], 0.0);
+    __syncthreads();
+  }
+  // explicit Q (zung2r)
+  for (int i = no - 1; i >= 0; --i) {
+    const double2 ti = tau[i];
+    if (i < no - 1) {
+      if (tid == 0) A[i * lda + i] = make_double2(1.0, 0.0);
+      __syncthreads();
+      const int nj = no - i - 1;
+      const int nrs = T / nj;
+      if (tid < nrs * nj) {
+        const int j = i + 1 + tid % nj, rs = tid / nj;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int p = i + rs; p < N; p += nrs) acc = cadd(acc, cmul(cconj(A[p * lda + i]), A[p * lda + j]));
+        wpart[tid] = acc;
+      }
+      __syncthreads();
+      for (int j = tid; j < nj; j += T) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int rs = 0; rs < nrs; ++rs) acc = cadd(acc, wpart[rs * nj + j]);
+        wv[j] = acc;
+      }
+      __syncthreads();
+      const int rows = N - i;
+      for (int e = tid; e < rows * nj; e += T) {
+        const int p = i + e / nj, j = e - (e / nj) * nj;
+        const double2 vp = A[p * lda + i];
+        A[p * lda + i + 1 + j] = csub(A[p * lda + i + 1 + j], cmul(ti, cmul(vp, wv[j])));
+      }
+      __syncthreads();
+    }
+    const double2 mt = make_double2(-ti.x, -ti.y);
+    for (int p = i + 1 + tid; p < N; p += T) A[p * lda + i] = cmul(A[p * lda + i], mt);
+    for (int p = tid; p < i; p += T) A[p * lda + i] = make_double2(0.0, 0.0);
+    if (tid == 0) A[i * lda + i] = make_double2(1.0 - ti.x, -ti.y);
+    __syncthreads();
+  }
+}
+
+// grid (W, ns).  use_smem: walker copied to shared memory with row stride no+1.
+__global__ void __launch_bounds__(kQrThreads)
+    qr_kernel(int N, int no0, int no1, double* w0, double* w1, int sign_fix, int use_smem,
+              double* sector_norm /* (ns, W) */) {
+  extern __shared__ double2 qsm[];
+  __shared__ double2 tau[64];
+  __shared__ double beta[64];
+  __shared__ double2 wv[64];
+  __shared__ double2 wpart[kQrThreads];
+  __shared__ double red[kQrThreads / 32];
+  __shared__ double2 scal_s;
+  const int w = blockIdx.x, s = blockIdx.y;
+  const int no = s ? no1 : no0;
+  double2* G = reinterpret_cast<double2*>(s ? w1 : w0) + (long long)w * N * no;
+  double2* A = G;
+  int lda = no;
+  if (use_smem) {
+    lda = no + 1;
+    A = qsm;
+    for (int e = threadIdx.x; e < N * no; e += kQrThreads) {
+      const int p = e / no, j = e - (e / no) * no;
+      A[p * lda + j] = G[e];
+    }
+    __syncthreads();
+  }
+  qr_inplace(A, lda, N, no, tau, beta, wv, wpart, red, &scal_s);
+  // prod diag R (real) and optional sign fix of column 0
+  __shared__ double prod_s;
+  if (threadIdx.x == 0) {
+    double pr = 1.0;
+    for (int k = 0; k < no; ++k) pr *= beta[k];
+    prod_s = pr;
+    if (sector_norm) sector_norm[(long long)s * gridDim.x + w] = pr;
+  }
+  __syncthreads();
+  const double sg = sign_fix ? ((prod_s > 0.0) ? 1.0 : ((prod_s < 0.0) ? -1.0 : 0.0)) : 1.0;
+  if (use_smem) {
+    for (int e = threadIdx.x; e < N * no; e += kQrThreads) {
+      const int p = e / no, j = e - (e / no) * no;
+      double2 v = A[p * lda + j];
+      if (j == 0) v = cscale(v, sg);
+      G[e] = v;
+    }
+  } else if (sign_fix) {
+    for (int p = threadIdx.x; p < N; p += kQrThreads) G[p * no] = cscale(G[p * no], sg);
+  }
+}
+
+__global__ void qr_norm_kernel(int W, int ns, int restricted, const double* sector_norm,
+                               double* norms) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  double n;
+  if (restricted)
+    n = sector_norm[w];
+  else
+    n = fabs(sector_norm[w]) * (ns == 2 ? fabs(sector_norm[W + w]) : 1.0);
+  norms[2 * w] = n;
+  norms[2 * w + 1] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// comb reconfiguration (single CTA); bit-exact: serial cumsum, explicit
+// round-to-nearest arithmetic in the reference's expression order.
+// ---------------------------------------------------------------------------
+__global__ void sr_kernel(int W, const double* win, double zeta, int mode, double* wout,
+                          int* idx) {
+  extern __shared__ double cum[];
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < W; ++i) {
+      s = __dadd_rn(s, fabs(win[i]));
+      cum[i] = s;
+    }
+  }
+  __syncthreads();
+  const double total = cum[W - 1];
+  const double dW = (double)W;
+  for (int i = threadIdx.x; i < W; i += blockDim.x) {
+    double z;
+    if (mode == AFQ_SR_LOCAL)
+      z = __ddiv_rn(__dmul_rn(total, __dadd_rn((double)i, zeta)), dW);
+    else
+      z = __dmul_rn(__ddiv_rn(__ddiv_rn(__dadd_rn((double)i, zeta), dW), 1.0), total);
+    int lo = 0, hi = W;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (cum[mid] < z)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    idx[i] = lo < W ? lo : W - 1;
+    wout[i] = (mode == AFQ_SR_LOCAL) ? __ddiv_rn(total, dW) : __ddiv_rn(__ddiv_rn(total, dW), 1.0);
+  }
+}
+
+__global__ void gather_kernel(long long wd2, const double2* in, double2* out, const int* idx) {
+  const int i = blockIdx.y;
+  const double2* src = in + (long long)idx[i] * wd2;
+  double2* dst = out + (long long)i * wd2;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < wd2;
+       e += (long long)gridDim.x * blockDim.x)
+    dst[e] = src[e];
+}
+
+// ---------------------------------------------------------------------------
+// block end: clamp, block energy/weight, population-control shift, killed count
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024)
+    block_end_kernel(int W, double dt, const double* wscal, const double* weights,
+                     double* scalars, double* block_out) {
+  __shared__ double red[3 * 32];
+  const double est = scalars[0];
+  const double thr = sqrt(2.0 / dt);
+  double swe = 0.0, sw = 0.0, nz = 0.0;
+  for (int w = threadIdx.x; w < W; w += blockDim.x) {
+    double e = wscal[(long long)w * 16 + 14];
+    if (fabs(e - est) > thr) e = est;
+    const double wt = weights[w];
+    swe += e * wt;
+    sw += wt;
+    nz += (wt != 0.0) ? 1.0 : 0.0;
+  }
+  swe = block_sum(swe, red);
+  sw = block_sum(sw, red + 32);
+  nz = block_sum(nz, red + 64);
+  if (threadIdx.x == 0) {
+    const double be = swe / sw;
+    block_out[0] = be;
+    block_out[1] = sw;
+    scalars[1] = 0.9 * scalars[1] + 0.1 * be;
+    scalars[2] += (double)W - nz;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) + Box-Muller
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox_round(uint4 c, uint2 k) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+  const uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+  return make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+}
+__device__ __forceinline__ uint4 philox10(uint4 c, uint2 k) {
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    c = philox_round(c, k);
+    k.x += W0;
+    k.y += W1;
+  }
+  return c;
+}
+__device__ __forceinline__ double u53(uint32_t hi, uint32_t lo) {
+  const unsigned long long x = ((unsigned long long)hi << 32) | lo;
+  return ((double)(x >> 11) + 0.5) * 0x1.0p-53;  // in (0, 1)
+}
+
+__global__ void normal_kernel(double* out, long long n, unsigned long long seed,
+                              unsigned long long offset) {
+  const long long npair = (n + 1) / 2;
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npair;
+       i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long ctr = offset + (unsigned long long)i;
+    const uint4 r = philox10(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), 0u, 0u), key);
+    const double u1 = u53(r.x, r.y), u2 = u53(r.z, r.w);
+    const double rad = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    out[2 * i] = rad * cs;
+    if (2 * i + 1 < n) out[2 * i + 1] = rad * sn;
+  }
+}
+
+__global__ void set_scalars_kernel(double* dst, double a, double b, double c, double d) {
+  dst[0] = a;
+  dst[1] = b;
+  dst[2] = c;
+  dst[3] = d;
+}
+
+}  // namespace
+
+cudaError_t launch_weight_update(const Layout& L, const double* prep, double* work,
+                                 double* weights, double* overlaps, double* scalars, double dt,
+                                 cudaStream_t st) {
+  ProfScope ps(K_WEIGHT, st);
+  weight_kernel<<<1, kWeightThreads, 0, st>>>(L.W, dt, prep + L.p_scal, work + L.w_wscal, weights,
+                                              overlaps, scalars);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_qr(const Layout& L, double* const walkers[2], double* norms, double* work,
+                      cudaStream_t st) {
+  const size_t smem = size_t(L.N) * (L.nomax + 1) * sizeof(double2);
+  const int use_smem = smem <= 200 * 1024;
+  const size_t dyn = use_smem ? smem : 0;
+  cudaError_t e =
+      cudaFuncSetAttribute(qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e != cudaSuccess) return e;
+  double* secn = work;  // (ns, W) doubles of scratch at the start of the workspace
+  dim3 grid(L.W, L.ns);
+  {
+    ProfScope ps(K_QR, st);
+    qr_kernel<<<grid, kQrThreads, dyn, st>>>(L.N, L.no[0], L.no[1], walkers[0],
+                                             L.ns == 2 ? walkers[1] : nullptr,
+                                             L.restricted ? 0 : 1, use_smem, secn);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess || !norms) return e;
+  ProfScope ps(K_MISC, st);
+  qr_norm_kernel<<<(L.W + 255) / 256, 256, 0, st>>>(L.W, L.ns, L.restricted, secn, norms);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sr(int W, const double* weights_in, double zeta, int mode,
+                      double* weights_out, int* indices, cudaStream_t st) {
+  const size_t smem = size_t(W) * sizeof(double);
+  cudaError_t e =
+      cudaFuncSetAttribute(sr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  ProfScope ps(K_SR, st);
+  sr_kernel<<<1, 1024, smem, st>>>(W, weights_in, zeta, mode, weights_out, indices);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather(int W, long long walker_doubles, const double* in, double* out,
+                          const int* indices, cudaStream_t st) {
+  const long long wd2 = walker_doubles / 2;
+  int bx = (int)((wd2 + 255) / 256);
+  if (bx > 64) bx = 64;
+  dim3 grid(bx, W);
+  ProfScope ps(K_GATHER, st);
+  gather_kernel<<<grid, 256, 0, st>>>(wd2, reinterpret_cast<const double2*>(in),
+                                      reinterpret_cast<double2*>(out), indices);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_block_end(const Layout& L, double* work, const double* weights,
+                             double* scalars, double dt, double* block_out, cudaStream_t st) {
+  ProfScope ps(K_BLOCKEND, st);
+  block_end_kernel<<<1, 1024, 0, st>>>(L.W, dt, work + L.w_wscal, weights, scalars, block_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_normal(double* out, long long n, unsigned long long seed,
+                          unsigned long long offset, cudaStream_t st) {
+  const long long npair = (n + 1) / 2;
+  long long blocks = (npair + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  ProfScope ps(K_NORMAL, st);
+  normal_kernel<<<(int)blocks, 256, 0, st>>>(out, n, seed, offset);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_set_scalars(double* dst, double a, double b, double c, double d,
+                               cudaStream_t st) {
+  ProfScope ps(K_MISC, st);
+  set_scalars_kernel<<<1, 1, 0, st>>>(dst, a, b, c, d);
+  return cudaGetLastError();
+}
+
+}  // namespace afq

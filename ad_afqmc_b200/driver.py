@@ -1,0 +1,74 @@
+"""Energy driver loop (mirror of ad_afqmc/driver.py:24-192 and :653-715, one rank).
+
+The control flow of ``afqmc_energy`` is kept: intermediates, initial
+propagation data, equilibration with a 50-step sampler, then ``n_blocks``
+calls of ``sampler.propagate_phaseless`` each followed by QR, the driver's
+(global-formula) reconfiguration and the e_estimate update.  Block energies
+stay FP64 (the reference casts to float32 for MPI at driver.py:138-139).
+The statistics (outlier rejection + blocking analysis) are host NumPy on the
+per-block scalars, as in stat_utils.py.
+"""
+
+from __future__ import annotations
+
+from typing import Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import stat_utils
+from .sampling import sampler as sampler_cls
+
+
+def _run_equilibration(ham, ham_data, prop, prop_data, trial, wave_data, sampler_eq,
+                       field_source=None):
+    """driver.py:653-715 (single rank)."""
+    for _ in range(sampler_eq.n_blocks):
+        e, prop_data = sampler_eq.propagate_phaseless(ham, ham_data, prop, prop_data, trial, wave_data)
+        prop_data["walkers"] = prop_data["walkers"].orthonormalize()
+        zeta = field_source.uniform() if field_source is not None else prop_data["key"].uniform()
+        prop_data["walkers"], prop_data["weights"] = prop_data["walkers"].stochastic_reconfiguration_global(
+            prop_data["weights"], zeta)
+        prop_data["e_estimate"] = 0.9 * prop_data["e_estimate"] + 0.1 * e
+    return prop_data
+
+
+def afqmc_blocks(ham, ham_data, prop, prop_data, trial, wave_data, smp, n_blocks,
+                 field_source=None):
+    """Sampling loop of driver.py:133-168 on one rank; returns (energies, weights, prop_data)."""
+    energies = torch.zeros(n_blocks, dtype=torch.float64, device=prop_data["weights"].device)
+    weights = torch.zeros_like(energies)
+    for n in range(n_blocks):
+        e, prop_data = smp.propagate_phaseless(ham, ham_data, prop, prop_data, trial, wave_data)
+        energies[n] = e
+        weights[n] = torch.sum(prop_data["weights"])
+        prop_data["walkers"] = prop_data["walkers"].orthonormalize()
+        zeta = field_source.uniform() if field_source is not None else prop_data["key"].uniform()
+        prop_data["walkers"], prop_data["weights"] = prop_data["walkers"].stochastic_reconfiguration_global(
+            prop_data["weights"], zeta)
+        prop_data["e_estimate"] = 0.9 * prop_data["e_estimate"] + 0.1 * e
+    return energies, weights, prop_data
+
+
+def afqmc_energy(ham_data: dict, ham, propagator, trial, wave_data: dict, sampler, options: dict,
+                 MPI=None, init_walkers=None, tmpdir: str = ".") -> Tuple[float, float]:
+    """driver.py:24-192 on one GPU (no MPI ranks)."""
+    if "rdm1" not in wave_data:
+        wave_data["rdm1"] = trial.get_rdm1(wave_data)
+    ham_data = ham.build_measurement_intermediates(ham_data, trial, wave_data)
+    ham_data = ham.build_propagation_intermediates(ham_data, propagator, trial, wave_data)
+    prop_data = propagator.init_prop_data(trial, wave_data, ham_data, options.get("seed", 0),
+                                          init_walkers)
+    if float(torch.abs(torch.sum(prop_data["overlaps"]))) < 1.0e-6:
+        raise ValueError("Initial overlaps are zero. Pass walkers with non-zero overlap.")
+    sampler_eq = sampler_cls(n_prop_steps=50, n_ene_blocks=options.get("n_ene_blocks_eql", 1),
+                             n_sr_blocks=options.get("n_sr_blocks_eql", 5),
+                             n_blocks=options.get("n_eql", 1))
+    prop_data = _run_equilibration(ham, ham_data, propagator, prop_data, trial, wave_data, sampler_eq)
+    energies, weights, prop_data = afqmc_blocks(ham, ham_data, propagator, prop_data, trial, wave_data,
+                                                sampler, sampler.n_blocks)
+    e = energies.cpu().numpy()
+    w = weights.cpu().numpy()
+    np.savetxt(tmpdir + "/samples_raw.dat", np.stack((w, e)).T)
+    clean, _ = stat_utils.reject_outliers(np.stack((w, e)).T, 1)
+    return stat_utils.blocking_analysis(clean[:, 0], clean[:, 1], neql=0)

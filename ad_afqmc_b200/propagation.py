@@ -1,0 +1,211 @@
+"""Phaseless propagator on the device (mirror of ad_afqmc/propagation.py).
+
+``propagator_afqmc`` keeps the reference's fields (propagation.py:111-121),
+``prop_data`` keys and method signatures: ``init_prop_data`` (:123-152),
+``propagate_constrained`` (:274-336) and
+``_build_propagation_intermediates`` (:378-438).  One call of
+``propagate_constrained`` is one C-ABI call (``afq_propagate_constrained``)
+that runs force bias, VHS, the Taylor propagator, overlaps and the weight
+update on the GPU.  Device-resident scalars (``e_estimate``,
+``pop_control_ene_shift``, the killed-walker count) live in
+``prop_data["_scalars"]`` so the step needs no host round trip.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Any, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._engine import device, drop_engines, get_engine, to_dev
+from .walkers import RHFWalkers, UHFWalkers
+
+
+class PRNGKey:
+    """Counter-based key replacing ``jax.random.PRNGKey`` (propagation.py:134).
+
+    ``seed`` selects the Philox stream; ``counter`` advances with every draw,
+    which plays the role of ``random.split``."""
+
+    def __init__(self, seed: int, counter: int = 0):
+        self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        self.counter = int(counter)
+
+    def take(self, n_pairs: int) -> int:
+        c = self.counter
+        self.counter += int(n_pairs)
+        return c
+
+    def uniform(self) -> float:
+        """One U(0,1) draw for reconfiguration (replaces random.uniform(subkey))."""
+        c = self.take(1)
+        return float(np.random.default_rng([self.seed, c, 0x5A5A]).random())
+
+    def __repr__(self):
+        return f"PRNGKey(seed={self.seed}, counter={self.counter})"
+
+
+def normal_fields(key: PRNGKey, shape, dev=None) -> torch.Tensor:
+    """Standard-normal float64 fields drawn on the device (afq_normal_fields)."""
+    n = int(np.prod(shape))
+    out = torch.empty(n, dtype=torch.float64, device=dev or device())
+    off = key.take((n + 1) // 2)
+    _lib.check(_lib.lib().afq_normal_fields(out.data_ptr(), n, key.seed, off, _lib.stream_handle()),
+               "afq_normal_fields")
+    return out.reshape(shape)
+
+
+def _scalar(v) -> torch.Tensor:
+    return to_dev(torch.as_tensor(v, dtype=torch.float64).reshape(()))
+
+
+def sync_scalars(prop_data: dict) -> torch.Tensor:
+    """Bind e_estimate / pop_control_ene_shift / n_killed_walkers to the device scalars."""
+    sc = prop_data.get("_scalars")
+    if sc is None:
+        sc = torch.zeros(8, dtype=torch.float64, device=device())
+        prop_data["_scalars"] = sc
+    for i, k in enumerate(("e_estimate", "pop_control_ene_shift", "n_killed_walkers")):
+        if k not in prop_data:
+            continue
+        v = prop_data[k]
+        view = sc[i]
+        if isinstance(v, torch.Tensor) and v.is_cuda and v.data_ptr() == view.data_ptr():
+            continue
+        view.copy_(_scalar(v))
+        prop_data[k] = view
+    for i, k in enumerate(("e_estimate", "pop_control_ene_shift", "n_killed_walkers")):
+        prop_data[k] = sc[i]
+    return sc
+
+
+def make_state(prop_data: dict) -> _lib.afq_state:
+    st = _lib.afq_state()
+    w = prop_data["walkers"]
+    if isinstance(w, UHFWalkers):
+        st.walkers[0] = w.data[0].data_ptr()
+        st.walkers[1] = w.data[1].data_ptr()
+    else:
+        st.walkers[0] = w.data.data_ptr()
+        st.walkers[1] = None
+    st.weights = prop_data["weights"].data_ptr()
+    st.overlaps = prop_data["overlaps"].data_ptr()
+    st.scalars = prop_data["_scalars"].data_ptr()
+    return st
+
+
+@dataclass
+class propagator:
+    dt: float = 0.01
+    n_walkers: int = 50
+
+
+@dataclass
+class propagator_afqmc(propagator):
+    """Propagator for phaseless AFQMC (propagation.py:111-441)."""
+
+    dt: float = 0.01
+    n_walkers: int = 50
+    n_exp_terms: int = 6
+    n_chunks: int = 1
+    vhs_real_dtype: Any = None
+    vhs_complex_dtype: Any = None
+    walker_type: str = "restricted"
+    precision: str = "fp64"
+
+    def engine(self, ham_data: dict, trial, wave_data: dict):
+        return get_engine(ham_data, trial, wave_data, self.walker_type, self.n_walkers, self.precision,
+                          self.dt, self.n_exp_terms)
+
+    def init_prop_data(self, trial, wave_data: dict, ham_data: dict, seed: int,
+                       init_walkers=None) -> dict:
+        """propagation.py:123-152."""
+        dev = device()
+        pd = {}
+        pd["weights"] = torch.ones(self.n_walkers, dtype=torch.float64, device=dev)
+        pd["key"] = PRNGKey(seed)
+        if init_walkers is not None:
+            if isinstance(init_walkers, (RHFWalkers, UHFWalkers)):
+                pd["walkers"] = init_walkers
+            elif isinstance(init_walkers, (list, tuple)):
+                pd["walkers"] = UHFWalkers(list(init_walkers))
+            else:
+                pd["walkers"] = RHFWalkers(init_walkers)
+        else:
+            pd["walkers"] = trial.get_init_walkers(wave_data, self.n_walkers, self.walker_type)
+        if "e_estimate" in ham_data:
+            pd["e_estimate"] = _scalar(ham_data["e_estimate"])
+        else:
+            e = torch.real(trial.calc_energy(pd["walkers"], ham_data, wave_data))
+            pd["e_estimate"] = torch.sum(e) / self.n_walkers
+        pd["pop_control_ene_shift"] = pd["e_estimate"].clone()
+        pd["n_killed_walkers"] = 0.0
+        sync_scalars(pd)
+        pd["overlaps"] = trial.calc_overlap(pd["walkers"], wave_data)
+        pd["normed_overlaps"] = pd["overlaps"]
+        pd["norms"] = torch.ones(self.n_walkers, dtype=torch.complex128, device=dev)
+        return pd
+
+    def propagate_constrained(self, trial, ham_data: dict, prop_data: dict, fields,
+                              wave_data: dict) -> dict:
+        """One phaseless step (propagation.py:274-336), in place on the device."""
+        eng = self.engine(ham_data, trial, wave_data)
+        if not eng.has_prop:
+            raise _lib.AfqError("propagation intermediates missing: call build_propagation_intermediates")
+        sync_scalars(prop_data)
+        f = to_dev(fields, torch.float64)
+        if f.shape != (self.n_walkers, int(ham_data["chol"].shape[0])):
+            raise ValueError(f"fields must be (n_walkers, nchol), got {tuple(f.shape)}")
+        st = make_state(prop_data)
+        p, w, wb = eng.handle
+        _lib.check(
+            _lib.lib().afq_propagate_constrained(C.byref(eng.dims), p, C.byref(st), f.data_ptr(), w, wb,
+                                                 _lib.stream_handle()),
+            "afq_propagate_constrained",
+        )
+        return prop_data
+
+    def _build_propagation_intermediates(self, ham_data: dict, trial, wave_data: dict) -> dict:
+        """mf_shifts, h0_prop, *_fp, exp_h1 (propagation.py:378-438), on the device."""
+        n = trial.norb
+        rdm1 = to_dev(wave_data["rdm1"])
+        rdm1 = rdm1[0] + rdm1[1]
+        ham_data["chol"] = to_dev(ham_data["chol"])
+        L = ham_data["chol"].reshape(-1, n, n)
+        G = L.shape[0]
+        mf = 1j * (ham_data["chol"] @ rdm1.reshape(-1)).to(torch.complex128)
+        ham_data["mf_shifts"] = mf
+        h0 = float(ham_data["h0"])
+        h0_prop = -h0 - torch.sum(mf**2) / 2.0
+        ham_data["h0_prop"] = h0_prop
+        na, nb = trial.nelec
+        ene0 = float(ham_data.get("ene0", 0.0))
+        if self.walker_type == "unrestricted":
+            ham_data["mf_shifts_fp"] = torch.stack((mf / na / 2.0, mf / nb / 2.0))
+            ham_data["h0_prop_fp"] = torch.stack(((h0_prop + ene0) / na / 2.0, (h0_prop + ene0) / nb / 2.0))
+        else:
+            ham_data["mf_shifts_fp"] = mf / 2.0 / na
+            ham_data["h0_prop_fp"] = (h0_prop + ene0) / na / 2.0
+        # v0 = 1/2 sum_g L_g L_g  as one GEMM over (g, k)
+        v0 = 0.5 * (L.permute(1, 0, 2).reshape(n, G * n) @ L.reshape(G * n, n))
+        mf_r = (1j * mf).real
+        v1 = (mf_r @ ham_data["chol"]).reshape(n, n)
+        h1 = to_dev(ham_data["h1"])
+        if self.walker_type == "unrestricted":
+            h1_mod = h1 - torch.stack([v0 + v1, v0 + v1])
+            ham_data["exp_h1"] = torch.stack([
+                torch.linalg.matrix_exp(-self.dt * h1_mod[0] / 2.0),
+                torch.linalg.matrix_exp(-self.dt * h1_mod[1] / 2.0),
+            ]).contiguous()
+        else:
+            h1_mod = (h1[0] + h1[1]) / 2.0 - v0 - v1
+            ham_data["exp_h1"] = torch.linalg.matrix_exp(-self.dt * h1_mod / 2.0).contiguous()
+        drop_engines(ham_data)
+        return ham_data
+
+    def __hash__(self) -> int:
+        return hash(tuple(str(v) for v in self.__dict__.values()))

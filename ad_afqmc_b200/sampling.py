@@ -1,0 +1,93 @@
+"""Block / reconfiguration loop on the device (mirror of ad_afqmc/sampling.py).
+
+``sampler.propagate_phaseless`` follows sampling.py:343-365 with the scans of
+``_sr_block_scan`` (:146-168), ``_block_scan`` (:52-94) and ``_step_scan``
+(:22-36) unrolled into C-ABI calls: one ``afq_propagate_constrained`` per
+step and one ``afq_block_end`` (QR, overlaps, energies, clamp, block energy,
+population shift) per energy block.  All state stays on the device; the
+returned energy is a 0-d CUDA tensor.
+
+Randomness: fields are drawn on the device from the counter-based key in
+``prop_data["key"]``.  A ``field_source`` object (with ``fields(S, W, G)``
+and ``uniform()``) replaces the device draws, which is how parity tests feed
+the same random numbers to this path and to the oracle.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Any, Optional
+
+import torch
+
+from . import _lib
+from ._engine import device, to_dev
+from .propagation import make_state, normal_fields, sync_scalars
+
+
+@dataclass
+class sampler:
+    n_prop_steps: int = 50
+    n_ene_blocks: int = 50
+    n_sr_blocks: int = 1
+    n_blocks: int = 50
+    field_source: Any = None
+
+    def _fields(self, prop, prop_data, nchol):
+        shape = (self.n_prop_steps, prop.n_walkers, nchol)
+        if self.field_source is not None:
+            return to_dev(self.field_source.fields(*shape), torch.float64)
+        return normal_fields(prop_data["key"], shape)
+
+    def _uniform(self, prop_data) -> float:
+        if self.field_source is not None:
+            return float(self.field_source.uniform())
+        return prop_data["key"].uniform()
+
+    def _block_scan(self, prop, trial, ham_data, prop_data, wave_data, out_row):
+        """sampling.py:52-94."""
+        eng = prop.engine(ham_data, trial, wave_data)
+        nchol = int(ham_data["chol"].shape[0])
+        fields = self._fields(prop, prop_data, nchol)
+        p, w, wb = eng.handle
+        lib = _lib.lib()
+        stream = _lib.stream_handle()
+        st = make_state(prop_data)
+        for s in range(self.n_prop_steps):
+            _lib.check(lib.afq_propagate_constrained(C.byref(eng.dims), p, C.byref(st),
+                                                     fields[s].data_ptr(), w, wb, stream),
+                       "afq_propagate_constrained")
+        _lib.check(lib.afq_block_end(C.byref(eng.dims), p, C.byref(st), out_row.data_ptr(), w, wb,
+                                     stream), "afq_block_end")
+
+    def propagate_phaseless(self, ham, ham_data: dict, prop, prop_data: dict, trial, wave_data: dict):
+        """sampling.py:343-365.  Returns (E, prop_data) with E a 0-d device tensor."""
+        eng = prop.engine(ham_data, trial, wave_data)
+        if not eng.has_prop:
+            raise _lib.AfqError("propagation intermediates missing: call build_propagation_intermediates")
+        prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+        prop_data["n_killed_walkers"] = 0.0
+        prop_data["pop_control_ene_shift"] = prop_data["e_estimate"]
+        if isinstance(prop_data["pop_control_ene_shift"], torch.Tensor):
+            prop_data["pop_control_ene_shift"] = prop_data["pop_control_ene_shift"].clone()
+        sync_scalars(prop_data)
+        nb = self.n_sr_blocks * self.n_ene_blocks
+        out = torch.zeros(nb, 2, dtype=torch.float64, device=device())
+        i = 0
+        for _ in range(self.n_sr_blocks):
+            for _ in range(self.n_ene_blocks):
+                self._block_scan(prop, trial, ham_data, prop_data, wave_data, out[i])
+                i += 1
+            zeta = self._uniform(prop_data)
+            prop_data["walkers"], prop_data["weights"] = prop_data[
+                "walkers"].stochastic_reconfiguration_local(prop_data["weights"], zeta)
+            prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+        sc = prop_data["_scalars"]
+        sc[2].div_(nb * prop.n_walkers)
+        be, bw = out[:, 0], out[:, 1]
+        prop_data["block_energies"] = out
+        return torch.sum(be * bw) / torch.sum(bw), prop_data
+
+    def __hash__(self) -> int:
+        return hash((self.n_prop_steps, self.n_ene_blocks, self.n_sr_blocks, self.n_blocks))

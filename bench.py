@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the phaseless AFQMC walker path (walker-steps/s).
+
+Workload (default): synthetic RHF Hamiltonian Norb=200, Na=Nb=40, Nchol=1000,
+512 walkers, dt=0.005 (see ad_afqmc_b200/synthetic.py for the recipe).  One
+bench step is one energy block of ``sampler.propagate_phaseless``: 10
+phaseless steps (device-drawn fields, force bias, VHS, Taylor propagator,
+overlaps, weights) followed by the block end (QR, overlaps, local energies,
+clamp, block energy, population shift) and one reconfiguration.  The metric
+counts walker-steps: 512 x 10 per bench step, with the per-block QR, energy
+and reconfiguration amortised inside the time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference ...   # the CPU oracle (NumPy port) arm
+
+Multi-GPU runs (torchrun, one process per GPU) are replicas: each rank runs
+its own walker population (weak scaling); the block energy and weight are
+combined with one NCCL all-reduce per block, the driver's only exchange.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "walker-steps/s @Norb200/Nchol1000 (mixed vs FP64 GPU, <=0.1 mHa); p99 solve latency"
+UNIT = "walker-steps/s"
+CONFIG = "rhf_n200_g1000"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--config", default=CONFIG)
+    ap.add_argument("--walkers", type=int, default=0, help="override walker count")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-walkers", type=int, default=32)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle timing (reported baseline; also the --impl reference arm)
+# ---------------------------------------------------------------------------
+def cpu_oracle_sample(sys_, n_walkers, n_steps, dt, seed=5):
+    """Time the NumPy oracle on a bounded sample: n_walkers walkers, n_steps
+    phaseless steps and one block end (QR + energies).  Returns walker-steps/s."""
+    from oracle import afqmc_oracle as orc
+
+    trial = orc.RHFTrial(sys_.norb, sys_.nelec) if sys_.trial == "rhf" else orc.UHFTrial(sys_.norb, sys_.nelec)
+    wt = "restricted" if sys_.trial == "rhf" else "unrestricted"
+    ham = sys_.ham_data()
+    wave = sys_.wave_data()
+    prop = orc.Propagator(dt=dt, n_walkers=n_walkers, walker_type=wt)
+    ham = trial.build_measurement_intermediates(ham, wave)
+    ham = prop.build_propagation_intermediates(ham, trial, wave)
+    rng = np.random.default_rng(seed)
+    pd = prop.init_prop_data(trial, wave, ham)
+    pd["n_killed_walkers"] = 0
+    fields = rng.standard_normal((n_steps, n_walkers, sys_.nchol))
+    t0 = time.perf_counter()
+    for s in range(n_steps):
+        pd = prop.propagate_constrained(trial, ham, pd, fields[s], wave)
+    pd["walkers"] = orc.orthonormalize(pd["walkers"])
+    pd["overlaps"] = trial.calc_overlap(pd["walkers"], wave)
+    e = np.real(trial.calc_energy(pd["walkers"], ham, wave))
+    idx, w = orc.sr_indices(pd["weights"], 0.5)
+    t = time.perf_counter() - t0
+    return n_walkers * n_steps / t, t
+
+
+def clocks_start(path):
+    try:
+        return subprocess.Popen(
+            ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+             "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except Exception:
+        return None
+
+
+def clocks_stop(proc, path, gpu_index):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except Exception:
+        proc.kill()
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9 or f[0] != str(gpu_index):
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx = float(f[2])
+        except ValueError:
+            continue
+        for n, v in zip(names, f[5:9]):
+            if v.lower() == "active":
+                reasons.add(n)
+    if not sm:
+        return None
+    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p)), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# FP64 dense peak of this pool's B200 (cuBLAS DGEMM 8192^3, measured with
+# CUDA events; the driver's peaks file carries no FP64 figure).
+FP64_PEAK_TFLOPS = 35.47
+
+
+def main():
+    args = parse()
+    from ad_afqmc_b200.synthetic import make_config
+
+    sys_, cfg = make_config(args.config)
+    W = args.walkers or cfg["n_walkers"]
+    S = cfg["n_prop_steps"]
+    dt = cfg["dt"]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        nw = max(8, args.cpu_walkers // 2)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, t = cpu_oracle_sample(sys_, nw, S, dt, seed=i)
+            if i >= args.warmup:
+                vals.append(v)
+        val = float(np.mean(vals))
+        cores = os.cpu_count()
+        out = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * nw * S / val,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic",
+               "config": {"workload": args.config, "norb": sys_.norb, "nelec": list(sys_.nelec),
+                          "nchol": sys_.nchol, "n_walkers": nw, "n_prop_steps": S, "dt": dt},
+               "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{nw} walkers x {S} steps + 1 block end (QR, energies, comb) "
+                                          "per step, NumPy oracle (the JAX reference needs jax, absent)"},
+               "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return 0
+
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    from ad_afqmc_b200 import _lib, hamiltonian, propagation, sampling, wavefunctions
+    from ad_afqmc_b200.driver import afqmc_blocks
+
+    trial = wavefunctions.rhf(sys_.norb, sys_.nelec) if sys_.trial == "rhf" else wavefunctions.uhf(sys_.norb, sys_.nelec)
+    wt = "restricted" if sys_.trial == "rhf" else "unrestricted"
+    ham_data, wave = sys_.ham_data(), sys_.wave_data()
+    ham = hamiltonian.hamiltonian(sys_.norb)
+    prop = propagation.propagator_afqmc(dt=dt, n_walkers=W, walker_type=wt, precision=args.precision)
+    ham_data = ham.build_measurement_intermediates(ham_data, trial, wave)
+    ham_data = ham.build_propagation_intermediates(ham_data, prop, trial, wave)
+    pd = prop.init_prop_data(trial, wave, ham_data, seed=1000 + rank)
+    smp = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1)
+
+    def one_block(pd, e_acc=None):
+        e, pd = smp.propagate_phaseless(ham, ham_data, prop, pd, trial, wave)
+        if world > 1:
+            t = torch.stack([e * torch.sum(pd["weights"]), torch.sum(pd["weights"])])
+            dist.all_reduce(t)
+        pd["e_estimate"] = 0.9 * pd["e_estimate"] + 0.1 * e
+        return pd, e
+
+    for _ in range(args.warmup):
+        pd, _ = one_block(pd)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    clk_path = os.path.join(tempfile.gettempdir(), f"afq_clocks_{rank}.csv")
+    clk = clocks_start(clk_path)
+    n0 = _lib.launch_count()
+    dominant = "vhs"
+    _lib.profile_begin(dominant)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    energies = []
+    for _ in range(args.steps):
+        pd, e = one_block(pd)
+        energies.append(e)
+    stop.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms_total = start.elapsed_time(stop)
+    kern_ms, kern_n = _lib.profile_end()
+    launches = _lib.launch_count() - n0
+    clocks = clocks_stop(clk, clk_path, torch.cuda.current_device())
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    value = world * W * S * args.steps / (ms_total / 1e3)
+    killed = float(pd["n_killed_walkers"])
+
+    # ---- end to end through the public API with host buffers -------------
+    e2e = None
+    if not args.no_e2e:
+        G = sys_.nchol
+        host_fields = torch.empty((S, W, G), dtype=torch.float64).pin_memory()
+        host_fields.normal_(generator=torch.Generator().manual_seed(7 + rank))
+
+        class PinnedSource:
+            def fields(self, s, w, g):
+                return host_fields.to(dev, non_blocking=True)
+
+            def uniform(self):
+                return 0.5
+
+        smp_e2e = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1, field_source=PinnedSource())
+        out_host = torch.empty(W + 1, dtype=torch.float64).pin_memory()
+
+        def e2e_block(pd):
+            e, pd = smp_e2e.propagate_phaseless(ham, ham_data, prop, pd, trial, wave)
+            out_host[0].copy_(e, non_blocking=True)
+            out_host[1:].copy_(pd["weights"], non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            pd["e_estimate"] = 0.9 * pd["e_estimate"] + 0.1 * e
+            return pd
+
+        pd = e2e_block(pd)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            pd = e2e_block(pd)
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([t_e2e], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        e2e = {"value": world * W * S * args.steps / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": int(host_fields.numel() * 8),
+               "d2h_bytes_per_step": int(out_host.numel() * 8)}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    # ---- roofline of the dominant kernel ------------------------------------
+    N, G = sys_.norb, sys_.nchol
+    flops_per_launch = 4.0 * W * N * N * G  # C(2W x N^2) = Xt(2W x G) L(G x N^2)
+    avg_ms = kern_ms / max(kern_n, 1)
+    achieved = flops_per_launch / (avg_ms / 1e3) / 1e12
+    if args.precision == "fp64":
+        peak, peak_src = FP64_PEAK_TFLOPS, "measured (cuBLAS DGEMM on this pool)"
+    else:
+        pk, src = measured_peaks()
+        peak, peak_src = pk["bf16_tflops"], src
+    roof = {"bound": "tensor", "kernel": "vhs_gemm_kernel", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_src,
+            "traffic": None, "launches": kern_n, "avg_launch_ms": avg_ms,
+            "flops_per_launch": flops_per_launch}
+
+    cpu = None
+    if not args.no_cpu:
+        v, t = cpu_oracle_sample(sys_, args.cpu_walkers, S, dt)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{args.cpu_walkers} walkers x {S} steps + 1 block end, NumPy oracle, "
+                         f"{t:.1f} s"}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3/f64",
+           "data": "synthetic",
+           "config": {"workload": args.config, "norb": N, "nelec": list(sys_.nelec), "nchol": G,
+                      "n_walkers_per_gpu": W, "n_prop_steps_per_bench_step": S, "dt": dt,
+                      "precision": args.precision, "parallelism": f"replicas x{world}",
+                      "l2": "working set (VHS 328 MB, chol 320 MB) exceeds the 126 MB L2",
+                      "killed_walker_fraction": killed},
+           "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+           "clocks": clocks}
+    print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,192 @@
+/*
+ * afqmc_b200.h -- C ABI of the B200 (sm_100a) phaseless-AFQMC walker path.
+ *
+ * One shared library, libafqmc_b200.so, exports the walker-path operations
+ * of ad_afqmc as plain C functions on raw device pointers.  The reference is
+ * pure Python/JAX and has no FFI of its own; each entry point below names the
+ * reference function (file:line inside the ad_afqmc project) whose behaviour
+ * it replaces, and the Python layer in ad_afqmc_b200/ binds them with ctypes
+ * behind the reference's method names.
+ *
+ * Conventions
+ *  - All array arguments are device pointers (CUDA global memory), 16-byte
+ *    aligned, C-contiguous.  complex128 data are interleaved (re, im) doubles.
+ *  - Walkers: restricted (W, N, No) complex128; unrestricted two arrays
+ *    (W, N, Na) and (W, N, Nb).
+ *  - exp_h1 and mf_shifts may be NULL in afq_prepare() when only
+ *    measurements (force bias, energy) are needed.
+ *  - Every function is asynchronous on the given stream (cudaStream_t passed
+ *    as void*; NULL = legacy default stream) and returns an afq_status.
+ *  - The library never allocates device memory.  Hamiltonian data are laid
+ *    out once by afq_prepare() into a caller-owned "prepared" buffer, and
+ *    every operation takes a caller-owned workspace; their sizes come from
+ *    afq_prepared_size() and afq_workspace_size().
+ *  - Calls on one workspace must not overlap on the device; distinct
+ *    (prepared, workspace) pairs are independent.
+ */
+#ifndef AFQMC_B200_H
+#define AFQMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum afq_status {
+  AFQ_OK = 0,
+  AFQ_ERR_SHAPE = 1,      /* unsupported or inconsistent sizes            */
+  AFQ_ERR_NULL = 2,       /* a required pointer is NULL                   */
+  AFQ_ERR_CUDA = 3,       /* CUDA runtime error during launch             */
+  AFQ_ERR_WORKSPACE = 4,  /* prepared/workspace buffer too small          */
+  AFQ_ERR_ALIGN = 5,      /* a pointer is not 16-byte aligned             */
+  AFQ_ERR_ARG = 6         /* an enum/flag argument is out of range        */
+} afq_status;
+
+enum { AFQ_RESTRICTED = 0, AFQ_UNRESTRICTED = 1 };      /* walker_type  */
+enum { AFQ_TRIAL_RHF = 0, AFQ_TRIAL_UHF = 1 };          /* trial_type   */
+enum { AFQ_FP64 = 0, AFQ_MIXED = 1 };                   /* precision    */
+enum { AFQ_SR_LOCAL = 0, AFQ_SR_GLOBAL = 1 };           /* sr z-formula */
+
+/* Problem sizes and method switches (fixed for one prepared buffer). */
+typedef struct afq_dims {
+  int32_t norb;        /* N: orbitals                                        */
+  int32_t nocc[2];     /* electrons per spin (restricted walkers use nocc[0]) */
+  int32_t nchol;       /* G: Cholesky vectors                                */
+  int32_t nwalkers;    /* W                                                  */
+  int32_t walker_type; /* AFQ_RESTRICTED / AFQ_UNRESTRICTED                  */
+  int32_t trial_type;  /* AFQ_TRIAL_RHF / AFQ_TRIAL_UHF                      */
+  int32_t n_exp_terms; /* Taylor terms incl. identity (reference default 6)  */
+  int32_t precision;   /* AFQ_FP64 / AFQ_MIXED                               */
+  int32_t reserved;    /* must be 0                                          */
+  double dt;           /* imaginary time step                                */
+} afq_dims;
+
+/* Trial and Hamiltonian inputs of afq_prepare() (device pointers). */
+typedef struct afq_ham {
+  const double* mo[2];       /* trial orbitals (N, nocc[s]) float64; [1] unused for RHF   */
+  const double* rot_h1[2];   /* (nocc[s], N) float64; RHF: [0] only                       */
+  const double* rot_chol[2]; /* (G, nocc[s], N) float64; RHF: [0] only                    */
+  const double* chol;        /* (G, N*N) float64                                          */
+  const double* exp_h1[2];   /* (N, N) float64; restricted walkers: [0] only              */
+  const double* mf_shifts;   /* (G,) complex128                                           */
+  double h0;                 /* constant energy                                           */
+  double h0_prop[2];         /* complex h0_prop (re, im)                                  */
+} afq_ham;
+
+/* Per-walker propagation state (device pointers, updated in place). */
+typedef struct afq_state {
+  double* walkers[2];  /* restricted: [0] (W,N,No); unrestricted: [0] up, [1] down  */
+  double* weights;     /* (W,) float64                                               */
+  double* overlaps;    /* (W,) complex128                                            */
+  double* scalars;     /* device doubles: [0] e_estimate, [1] pop_control_ene_shift,
+                          [2] n_killed_walkers (accumulated), [3..7] reserved       */
+} afq_state;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int afq_version(void);
+/* Human-readable status text. */
+const char* afq_status_string(int status);
+
+/* Bytes of the prepared Hamiltonian buffer / of the workspace. */
+int afq_prepared_size(const afq_dims* d, size_t* bytes);
+int afq_workspace_size(const afq_dims* d, size_t* bytes);
+
+/* Lay out trial + Hamiltonian intermediates for the kernels.
+ * Replaces the consumer side of rhf._build_measurement_intermediates
+ * (wavefunctions.py:1215-1232), uhf (:1472-1496) and
+ * propagator_afqmc._build_propagation_intermediates (propagation.py:378-438):
+ * those tensors are computed by the caller and copied here into padded,
+ * concatenated device layouts. */
+int afq_prepare(const afq_dims* d, const afq_ham* h, void* prepared, size_t prepared_bytes,
+                void* stream);
+
+/* Bytes of workspace needed by afq_calc_overlap / afq_calc_green /
+ * afq_orthonormalize (16 doubles per walker; no Hamiltonian data needed). */
+int afq_small_workspace_size(const afq_dims* d, size_t* bytes);
+
+/* overlap <psi_T|walker>  (W,) complex128.  mo: trial orbitals (N, nocc[s])
+ * float64 per spin ([1] ignored for an RHF trial).
+ * Replaces wave_function.calc_overlap (wavefunctions.py:93-200) ->
+ * rhf._calc_overlap_restricted (:1064-1066) / _unrestricted (:1068-1074),
+ * uhf._calc_overlap_unrestricted (:1259-1268). */
+int afq_calc_overlap(const afq_dims* d, const double* const mo[2], const double* const walkers[2],
+                     double* overlaps, void* work, size_t work_bytes, void* stream);
+
+/* half-rotated Green's function per spin, (W, nocc[s], N) complex128 each.
+ * Replaces rhf._calc_green (wavefunctions.py:1089-1100), uhf._calc_green (:1289-1312). */
+int afq_calc_green(const afq_dims* d, const double* const mo[2], const double* const walkers[2],
+                   double* const green[2], void* work, size_t work_bytes, void* stream);
+
+/* force bias (W, G) complex128.
+ * Replaces wave_function.calc_force_bias (wavefunctions.py:202-262) ->
+ * rhf._calc_force_bias_restricted (:1102-1110) / _unrestricted (:1112-1126),
+ * uhf._calc_force_bias_unrestricted (:1314-1329). */
+int afq_calc_force_bias(const afq_dims* d, const void* prepared, const double* const walkers[2],
+                        double* force_bias, void* work, size_t work_bytes, void* stream);
+
+/* local energy (W,) complex128.
+ * Replaces wave_function.calc_energy (wavefunctions.py:264-394) ->
+ * rhf._calc_energy_restricted (:1128-1141) / _unrestricted (:1143-1174),
+ * uhf._calc_energy_unrestricted (:1331-1363).  The exchange term is a fused
+ * kernel: the (G, No, No) intermediate is never written. */
+int afq_calc_energy(const afq_dims* d, const void* prepared, const double* const walkers[2],
+                    double* energies, void* work, size_t work_bytes, void* stream);
+
+/* One phaseless step: force bias, field shifts, VHS, Taylor propagator with
+ * one-body half-steps, new overlaps, phaseless weight update and population
+ * control shift.  fields: (W, G) float64 (device).
+ * Replaces propagator_afqmc.propagate_constrained (propagation.py:274-336)
+ * with _apply_trotprop* (:154-272). */
+int afq_propagate_constrained(const afq_dims* d, const void* prepared, afq_state* s,
+                              const double* fields, void* work, size_t work_bytes, void* stream);
+
+/* Householder QR of every walker in place (LAPACK zgeqrf/zungqr convention);
+ * norms (W,) complex128 (prod diag R; unrestricted: |.| per spin multiplied),
+ * may be NULL.  work: afq_small_workspace_size() bytes.  Unrestricted walkers get column 0 times sign(prod diag R).
+ * Replaces linalg_utils.qr_vmap_restricted / _unrestricted (linalg_utils.py:51-72)
+ * via RHFWalkers/UHFWalkers.orthonormalize (walkers.py:155-157, 260-262). */
+int afq_orthonormalize(const afq_dims* d, double* const walkers[2], double* norms, void* work,
+                       size_t work_bytes, void* stream);
+
+/* Comb resampling: indices (W,) int32 and new weights from weights and zeta;
+ * the walkers are gathered from walkers_in into walkers_out (distinct buffers).
+ * mode AFQ_SR_LOCAL follows sr.py:24-48, AFQ_SR_GLOBAL the single-rank
+ * rank-0 arithmetic of sr.py:52-153.  Serial FP64 cumsum: bit-exact indices
+ * given identical weights and zeta. */
+int afq_stochastic_reconfiguration(const afq_dims* d, const double* weights_in, double zeta,
+                                   int mode, const double* const walkers_in[2],
+                                   double* const walkers_out[2], double* weights_out,
+                                   int32_t* indices, void* stream);
+
+/* Block end of sampler._block_scan (sampling.py:76-94): killed-walker count,
+ * QR, overlaps, local energies with the sqrt(2/dt) clamp, block energy and
+ * weight, and the population-control shift update.
+ * block_out: device doubles [0] block energy, [1] block weight. */
+int afq_block_end(const afq_dims* d, const void* prepared, afq_state* s, double* block_out,
+                  void* work, size_t work_bytes, void* stream);
+
+/* Standard-normal auxiliary fields (n, ) float64 from a counter-based
+ * Philox4x32-10 generator with Box-Muller; (seed, offset) select the stream.
+ * Replaces random.normal(subkey, (S, W, G)) in sampler._block_scan
+ * (sampling.py:63-71); the bits differ from JAX threefry by design. */
+int afq_normal_fields(double* out, int64_t n, uint64_t seed, uint64_t offset, void* stream);
+
+/* Instrumentation (no counterpart in the reference, which has no native
+ * code): launches of one kernel family (kernel_id >= 0) or of all library
+ * kernels (kernel_id < 0) since load; and CUDA-event timing of every launch
+ * of one family between afq_profile_begin and afq_profile_end (events are
+ * recorded on the stream of each launch).  Families: 0 green, 1 force-bias
+ * GEMM, 2 field prep, 3 VHS GEMM, 4 propagator GEMMs, 5 exchange, 6 energy
+ * combine, 7 weights, 8 QR, 9 reconfiguration, 10 gather, 11 block end,
+ * 12 normal fields, 13 other. */
+int afq_launch_count(int kernel_id, unsigned long long* count);
+int afq_profile_begin(int kernel_id);
+int afq_profile_end(double* total_ms, int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AFQMC_B200_H */
