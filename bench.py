@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-walkers", type=int, default=32)
+    ap.add_argument("--chol-scale", type=float, default=1.0,
+                    help="Cholesky scale of the synthetic system (1.0 = prescribed recipe)")
     return ap.parse_args()
 
 
@@ -139,7 +141,7 @@ def main():
     args = parse()
     from ad_afqmc_b200.synthetic import make_config
 
-    sys_, cfg = make_config(args.config)
+    sys_, cfg = make_config(args.config, chol_scale=args.chol_scale)
     W = args.walkers or cfg["n_walkers"]
     S = cfg["n_prop_steps"]
     dt = cfg["dt"]
@@ -311,7 +313,7 @@ def main():
                       "n_walkers_per_gpu": W, "n_prop_steps_per_bench_step": S, "dt": dt,
                       "precision": args.precision, "parallelism": f"replicas x{world}",
                       "l2": "working set (VHS 328 MB, chol 320 MB) exceeds the 126 MB L2",
-                      "killed_walker_fraction": killed},
+                      "chol_scale": args.chol_scale, "killed_walker_fraction": killed},
            "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
            "clocks": clocks}
     print(json.dumps(out))
