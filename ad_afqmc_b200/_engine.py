@@ -18,6 +18,9 @@ from ._lib import AfqError
 
 CACHE_KEY = "_afq_engines"
 
+# precision switch of the walker path (see include/afqmc_b200.h)
+PRECISIONS = {"fp64": 0, "mixed": 1, "mixed_hi": 2}
+
 _small_work: Dict[Tuple, torch.Tensor] = {}
 
 
@@ -55,7 +58,7 @@ def dims_for(trial, walker_type: str, nwalkers: int, nchol: int = 1, precision: 
 
     wt = _lib.AFQ_RESTRICTED if walker_type == "restricted" else _lib.AFQ_UNRESTRICTED
     tt = _lib.AFQ_TRIAL_UHF if isinstance(trial, uhf) else _lib.AFQ_TRIAL_RHF
-    pr = _lib.AFQ_MIXED if precision == "mixed" else _lib.AFQ_FP64
+    pr = PRECISIONS[precision]
     return _lib.make_dims(trial.norb, trial.nelec, nchol, nwalkers, wt, tt, n_exp_terms, pr, dt)
 
 
@@ -67,7 +70,8 @@ class Engine:
         pbytes, wbytes = _lib.sizes(dims)
         dev = device()
         self.prepared = torch.empty(pbytes // 8, dtype=torch.float64, device=dev)
-        self.work = torch.empty(wbytes // 8, dtype=torch.float64, device=dev)
+        # zero-filled once: holds the device error flag of the tensor-core kernels
+        self.work = torch.zeros(wbytes // 8, dtype=torch.float64, device=dev)
         self.work_bytes = wbytes
         self.block_out = torch.zeros(2, dtype=torch.float64, device=dev)
         self._keep = []

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(_PKG, "lib", "libafqmc_b200.so")
 AFQ_OK = 0
 AFQ_RESTRICTED, AFQ_UNRESTRICTED = 0, 1
 AFQ_TRIAL_RHF, AFQ_TRIAL_UHF = 0, 1
-AFQ_FP64, AFQ_MIXED = 0, 1
+AFQ_FP64, AFQ_MIXED, AFQ_MIXED_HI = 0, 1, 2
 AFQ_SR_LOCAL, AFQ_SR_GLOBAL = 0, 1
 
 _dp = C.POINTER(C.c_double)
@@ -83,6 +83,10 @@ _SIGS = {
     "afq_stochastic_reconfiguration": ([C.POINTER(afq_dims), C.c_void_p, C.c_double, C.c_int, C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "afq_block_end": ([C.POINTER(afq_dims), C.c_void_p, C.POINTER(afq_state), C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
     "afq_normal_fields": ([C.c_void_p, C.c_int64, C.c_uint64, C.c_uint64, C.c_void_p], C.c_int),
+    "afq_split_bf16": ([C.c_void_p, C.c_int64, C.c_int, C.c_void_p * 3, C.c_void_p], C.c_int),
+    "afq_gemm_split_bf16": ([C.c_void_p * 3, C.c_int, C.c_void_p * 3, C.c_int, C.c_int, C.c_void_p,
+                             C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64,
+                             C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p], C.c_int),
     "afq_launch_count": ([C.c_int, C.POINTER(C.c_ulonglong)], C.c_int),
     "afq_profile_begin": ([C.c_int], C.c_int),
     "afq_profile_end": ([C.POINTER(C.c_double), C.POINTER(C.c_int)], C.c_int),
@@ -159,6 +163,52 @@ def pair(a, b=None):
 def stream_handle(stream: Optional[torch.cuda.Stream] = None) -> int:
     s = stream if stream is not None else torch.cuda.current_stream()
     return s.cuda_stream
+
+
+def triple(a=None, b=None, c=None):
+    arr = (C.c_void_p * 3)()
+    arr[0], arr[1], arr[2] = a, b, c
+    return arr
+
+
+def split_bf16(x: torch.Tensor, npieces: int):
+    """bf16 pieces of a float64 CUDA tensor (same shape each)."""
+    x = x.contiguous()
+    outs = [torch.empty(x.shape, dtype=torch.bfloat16, device=x.device) for _ in range(npieces)]
+    ptrs = triple(*[o.data_ptr() for o in outs])
+    check(lib().afq_split_bf16(x.data_ptr(), x.numel(), npieces, ptrs, stream_handle()), "afq_split_bf16")
+    return outs
+
+
+BF16X3 = ((0, 0), (0, 1), (1, 0))
+BF16X6 = ((0, 0), (0, 1), (1, 0), (0, 2), (1, 1), (2, 0))
+
+
+def gemm_split_bf16(a_pieces, b_pieces, pairs, out=None):
+    """C[b] = sum_pairs A_i[b] @ B_j[b]^T for (batch, rows, K) bf16 pieces."""
+    a0, b0 = a_pieces[0], b_pieces[0]
+    if a0.dim() == 2:
+        a_pieces = [a.unsqueeze(0) for a in a_pieces]
+        b_pieces = [b.unsqueeze(0) for b in b_pieces]
+        a0, b0 = a_pieces[0], b_pieces[0]
+        squeeze = True
+    else:
+        squeeze = False
+    batch, M, K = a0.shape
+    N = b0.shape[1]
+    if out is None:
+        out = torch.empty(batch, M, N, dtype=torch.float32, device=a0.device)
+    pr = torch.tensor([v for p in pairs for v in p], dtype=torch.int32)
+    err = torch.zeros(1, dtype=torch.int32, device=a0.device)
+    rc = lib().afq_gemm_split_bf16(
+        triple(*[a.data_ptr() for a in a_pieces]), len(a_pieces),
+        triple(*[b.data_ptr() for b in b_pieces]), len(b_pieces), len(pairs),
+        pr.data_ptr(), M, N, K, batch, a0.stride(1), a0.stride(0), b0.stride(1), b0.stride(0),
+        out.data_ptr(), out.stride(1), out.stride(0), err.data_ptr(), stream_handle())
+    check(rc, "afq_gemm_split_bf16")
+    if int(err.item()) != 0:
+        raise AfqError("afq_gemm_split_bf16: a device wait timed out")
+    return out[0] if squeeze else out
 
 
 def make_dims(norb, nocc, nchol, nwalkers, walker_type, trial_type, n_exp_terms, precision, dt):

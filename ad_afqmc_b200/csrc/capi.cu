@@ -55,7 +55,12 @@ GreenArgs green_args_mo(const Layout& L, const double* const mo[2], double* work
     a.sec[s].koff = L.koff[s];
     a.sec[s].theta = nullptr;
     a.sec[s].gout = nullptr;
+    for (int i = 0; i < 3; ++i) a.sec[s].gtb[i] = nullptr;
+    a.sec[s].ldtb = L.Nb;
   }
+  a.npc = L.npc;
+  for (int i = 0; i < 3; ++i) a.gplb[i] = nullptr;
+  a.ldgb = L.Kb;
   return a;
 }
 
@@ -74,16 +79,40 @@ int check_small(const afq_dims* d, Layout& L, void* work, size_t work_bytes) {
   return AFQ_OK;
 }
 
+// Green's function of the current walkers and the force-bias contraction
+// (split-K partial sums in the workspace, consumed by the field preparation).
+int force_bias_impl(const Layout& L, const double* prep, double* work, GreenArgs& a,
+                    cudaStream_t st) {
+  if (L.mixed)
+    piece_ptrs(work, L.v_gpl, L.v_gpl_ps, L.npc, a.gplb);
+  else
+    a.gpl = work + L.w_gpl;
+  AFQ_TRY(launch_green(a, st));
+  if (L.mixed) return mixed_fb_gemm(L, prep, work, st);
+  AFQ_TRY(launch_fb_gemm(L, prep, work, st));
+  return AFQ_OK;
+}
+
 // energy of the current walkers into wscal[.,14..15] and optionally eout
 int energy_impl(const Layout& L, const double* prep, double* work, const double* const walkers[2],
                 double* eout, int eout_stride, cudaStream_t st) {
   GreenArgs a = green_args(L, prep, work, walkers);
   for (int s = 0; s < L.ns; ++s) {
-    a.sec[s].theta = work + L.w_theta[s];
     a.sec[s].rh1 = prep + L.p_rh1[s];
+    if (L.mixed)
+      piece_ptrs(work, L.v_gt[s], L.v_gt_ps[s], L.npc, a.sec[s].gtb);
+    else
+      a.sec[s].theta = work + L.w_theta[s];
   }
   AFQ_TRY(launch_green(a, st));
-  for (int s = 0; s < L.ns; ++s) AFQ_TRY(launch_exchange(L, prep, work, s, st));
+  for (int s = 0; s < L.ns; ++s) {
+    if (L.mixed) {
+      const int rc = mixed_exchange(L, prep, work, s, st);
+      if (rc != AFQ_OK) return rc;
+    } else {
+      AFQ_TRY(launch_exchange(L, prep, work, s, st));
+    }
+  }
   AFQ_TRY(launch_energy_combine(L, prep, work, eout, eout_stride, st));
   return AFQ_OK;
 }
@@ -167,6 +196,7 @@ int afq_prepare(const afq_dims* d, const afq_ham* h, void* prepared, size_t prep
     AFQ_TRY(cudaMemcpyAsync(P + L.p_mf, h->mf_shifts, (size_t)L.G * 2 * D, cudaMemcpyDeviceToDevice,
                           st));
   AFQ_TRY(launch_set_scalars(P + L.p_scal, h->h0, h->h0_prop[0], h->h0_prop[1], 0.0, st));
+  if (L.mixed) return mixed_prepare(L, P, st);
   return AFQ_OK;
 }
 
@@ -222,9 +252,8 @@ int afq_calc_force_bias(const afq_dims* d, const void* prepared, const double* c
   double* Wk = static_cast<double*>(work);
   cudaStream_t st = as_stream(stream);
   GreenArgs a = green_args(L, P, Wk, walkers);
-  a.gpl = Wk + L.w_gpl;
-  AFQ_TRY(launch_green(a, st));
-  AFQ_TRY(launch_fb_gemm(L, P, Wk, st));
+  rc = force_bias_impl(L, P, Wk, a, st);
+  if (rc != AFQ_OK) return rc;
   AFQ_TRY(launch_prep(L, P, Wk, nullptr, d->dt, force_bias, st));
   return AFQ_OK;
 }
@@ -254,13 +283,18 @@ int afq_propagate_constrained(const afq_dims* d, const void* prepared, afq_state
   cudaStream_t st = as_stream(stream);
   // force bias of the current walkers
   GreenArgs a = green_args(L, P, Wk, wc);
-  a.gpl = Wk + L.w_gpl;
-  AFQ_TRY(launch_green(a, st));
-  AFQ_TRY(launch_fb_gemm(L, P, Wk, st));
+  rc = force_bias_impl(L, P, Wk, a, st);
+  if (rc != AFQ_OK) return rc;
   AFQ_TRY(launch_prep(L, P, Wk, fields, d->dt, nullptr, st));
   // VHS and the Trotterized propagator
-  AFQ_TRY(launch_vhs_gemm(L, P, Wk, st));
-  AFQ_TRY(launch_propagate_walkers(L, P, Wk, s->walkers, d->n_exp_terms, st));
+  if (L.mixed) {
+    if ((rc = mixed_vhs_gemm(L, P, Wk, st)) != AFQ_OK) return rc;
+    if ((rc = mixed_propagate_walkers(L, P, Wk, s->walkers, d->n_exp_terms, st)) != AFQ_OK)
+      return rc;
+  } else {
+    AFQ_TRY(launch_vhs_gemm(L, P, Wk, st));
+    AFQ_TRY(launch_propagate_walkers(L, P, Wk, s->walkers, d->n_exp_terms, st));
+  }
   // new overlaps and the phaseless weight update
   GreenArgs b = green_args(L, P, Wk, wc);
   AFQ_TRY(launch_green(b, st));

@@ -1,6 +1,7 @@
 // Shared device helpers for the phaseless-AFQMC walker kernels (sm_100a).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -61,6 +62,35 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(d0), "+d"(d1)
                : "d"(a), "d"(b));
+}
+
+// ---------------------------------------------------------------------------
+// bf16 operand pieces: x ~= p0 + p1 (+ p2), each rounded to nearest from the remainder
+// ---------------------------------------------------------------------------
+typedef __nv_bfloat16 bf16;
+
+__device__ __forceinline__ void put_pieces(double x, int np, bf16* const* P, long long idx) {
+  const bf16 a = __double2bfloat16(x);
+  P[0][idx] = a;
+  double r = x - (double)__bfloat162float(a);
+  const bf16 b = __double2bfloat16(r);
+  P[1][idx] = b;
+  if (np > 2) {
+    r -= (double)__bfloat162float(b);
+    P[2][idx] = __double2bfloat16(r);
+  }
+}
+
+__device__ __forceinline__ void put_pieces_f(float x, int np, bf16* const* P, long long idx) {
+  const bf16 a = __float2bfloat16_rn(x);
+  P[0][idx] = a;
+  float r = x - __bfloat162float(a);
+  const bf16 b = __float2bfloat16_rn(r);
+  P[1][idx] = b;
+  if (np > 2) {
+    r -= __bfloat162float(b);
+    P[2][idx] = __float2bfloat16_rn(r);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -62,7 +62,9 @@ __global__ void __launch_bounds__(256) prep_kernel(int W, int G, long long Gpad,
                                                    const double* fbpart, double alpha,
                                                    const double* fields, const double* mf,
                                                    double sdt, double* xt, double* wscal,
-                                                   double* fb_out) {
+                                                   double* fb_out, int npc, bf16* xb0, bf16* xb1,
+                                                   bf16* xb2, long long ldxb) {
+  bf16* const xb[3] = {xb0, xb1, xb2};
   __shared__ double red[4 * 8];
   const int w = blockIdx.x, tid = threadIdx.x;
   const long long zs = 2LL * W * Gpad;
@@ -91,8 +93,13 @@ __global__ void __launch_bounds__(256) prep_kernel(int W, int G, long long Gpad,
       br += x * fsr - (fsr * fsr - fsi * fsi) / 2.0;
       bi += x * fsi - (2.0 * fsr * fsi) / 2.0;
       // VHS = i sqrt(dt) x~ L  ->  rows (w,0)=Re VHS, (w,1)=Im VHS
-      xt[(2LL * w) * Gpad + g] = -sdt * xi;
-      xt[(2LL * w + 1) * Gpad + g] = sdt * xr;
+      if (xb0) {
+        put_pieces(-sdt * xi, npc, xb, (2LL * w) * ldxb + g);
+        put_pieces(sdt * xr, npc, xb, (2LL * w + 1) * ldxb + g);
+      } else {
+        xt[(2LL * w) * Gpad + g] = -sdt * xi;
+        xt[(2LL * w + 1) * Gpad + g] = sdt * xr;
+      }
     }
   }
   if (fields) {
@@ -344,9 +351,12 @@ cudaError_t launch_fb_gemm(const Layout& L, const double* prep, double* work, cu
 cudaError_t launch_prep(const Layout& L, const double* prep, double* work, const double* fields,
                         double dt, double* fb_out, cudaStream_t st) {
   ProfScope ps(K_PREP, st);
+  bf16* xb[3] = {nullptr, nullptr, nullptr};
+  if (L.mixed) piece_ptrs(work, L.v_xt, L.v_xt_ps, L.npc, xb);
   prep_kernel<<<L.W, 256, 0, st>>>(L.W, L.G, L.Gpad, L.splitk, work + L.w_fbpart,
                                    (double)L.mult, fields, prep + L.p_mf, sqrt(dt),
-                                   work + L.w_xt, work + L.w_wscal, fb_out);
+                                   work + L.w_xt, work + L.w_wscal, fb_out, L.npc, xb[0], xb[1],
+                                   xb[2], L.Gb);
   return cudaGetLastError();
 }
 

@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
     a.wscal[(long long)w * 16 + 5 + 2 * sct] = det.y;
   }
 
-  const bool need_theta = S_.theta || S_.gout || a.gpl || S_.rh1;
+  const bool need_theta = S_.theta || S_.gout || a.gpl || S_.rh1 || a.gplb[0] || S_.gtb[0];
   if (!need_theta) return;
 
   // ---- Theta = W S^-1, transposed copies, E1 --------------------------------
@@ -153,6 +153,8 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
   double2* go = S_.gout ? reinterpret_cast<double2*>(S_.gout) + (long long)w * no * N : nullptr;
   double* gre = a.gpl ? a.gpl + (2LL * w) * a.ldg + S_.koff : nullptr;
   double* gim = a.gpl ? a.gpl + (2LL * w + 1) * a.ldg + S_.koff : nullptr;
+  const bool gb = a.gplb[0] != nullptr;
+  const bool tb = S_.gtb[0] != nullptr;
   for (int p0 = 0; p0 < N; p0 += kRowChunk) {
     const int rows = min(kRowChunk, N - p0);
     for (int e = tid; e < rows * no; e += T) {
@@ -174,7 +176,7 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
       }
     }
     __syncthreads();
-    if (go || gre) {
+    if (go || gre || gb || tb) {
       for (int e = tid; e < rows * no; e += T) {
         const int j = e / rows, r = e - (e / rows) * rows;
         const double2 v = stage[r * no + j];
@@ -182,6 +184,16 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
         if (gre) {
           gre[(long long)j * N + p0 + r] = v.x;
           gim[(long long)j * N + p0 + r] = v.y;
+        }
+        if (gb) {
+          const long long o = S_.koff + (long long)j * N + p0 + r;
+          put_pieces(v.x, a.npc, a.gplb, (2LL * w) * a.ldgb + o);
+          put_pieces(v.y, a.npc, a.gplb, (2LL * w + 1) * a.ldgb + o);
+        }
+        if (tb) {
+          const long long rr = (long long)w * 2 * no + 2 * j;
+          put_pieces(v.x, a.npc, S_.gtb, rr * S_.ldtb + p0 + r);
+          put_pieces(v.y, a.npc, S_.gtb, (rr + 1) * S_.ldtb + p0 + r);
         }
       }
     }

@@ -24,9 +24,45 @@ struct ExchTile {
   int mt;   // number of row tiles = ceil(G / gpt)
 };
 
+// Exchange tile of the tensor-core path: 128 rows hold gpt Cholesky
+// vectors, BN columns hold wpt walkers.
+struct UExchTile {
+  int bn, gpt, wpt, mt;
+};
+
+// Largest column tile that holds whole walkers and leaves room for two
+// pipeline stages plus the epilogue's staging of one walker's f block.
+inline UExchTile choose_uexch_tile(int no, int G, int npc) {
+  UExchTile t;
+  const int bns[4] = {240, 160, 128, 80};
+  const long long budget = 227 * 1024 - 1024 - 256;
+  const long long extra = ((128LL * (2 * no + 1) * 4 + 31) & ~31LL) + 128 * 32 + 128 * 16;
+  t.bn = 0;
+  for (int i = 0; i < 4 && !t.bn; ++i) {
+    const int bn = bns[i];
+    if (((2 * no + 15) & ~15) > bn) continue;
+    const long long stage = (long long)npc * (128 * 128 + bn * 128);
+    if (2 * stage + extra <= budget) t.bn = bn;
+  }
+  t.gpt = 128 / no;
+  t.wpt = t.bn ? t.bn / (2 * no) : 0;
+  t.mt = (G + t.gpt - 1) / t.gpt;
+  return t;
+}
+
+inline long long round8(long long x) { return (x + 7) & ~7LL; }
+
 struct Layout {
   // sizes
   int N, G, W, no[2], ns, np, mult, restricted, uhf_trial, nomax;
+  int mixed, npc;      // tensor-core path and bf16 pieces per operand (2 or 3)
+  long long Kb, Gb, Nb, Kv;  // bf16 row strides (multiples of 8 elements)
+  UExchTile uex[2];
+  // bf16 buffers, offsets in doubles (4 bf16 per double); [piece] stride given by *_ps
+  long long q_rccat, q_cholT, q_exph1[2], q_rc[2];
+  long long q_rccat_ps, q_cholT_ps, q_exph1_ps, q_rc_ps[2];
+  long long v_gpl, v_xt, v_vhs, v_bt[2], v_acc, v_gt[2];
+  long long v_gpl_ps, v_xt_ps, v_vhs_ps, v_bt_ps, v_gt_ps[2];
   long long Npad, N2pad, Gpad, Kfb, Kfb_used, koff[2];
   int splitk;
   ExchTile ex[2];
@@ -60,7 +96,8 @@ inline int make_layout(const afq_dims* d, Layout& L) {
   if (d->norb <= 0 || d->nchol <= 0 || d->nwalkers <= 0) return AFQ_ERR_SHAPE;
   if (d->walker_type != AFQ_RESTRICTED && d->walker_type != AFQ_UNRESTRICTED) return AFQ_ERR_ARG;
   if (d->trial_type != AFQ_TRIAL_RHF && d->trial_type != AFQ_TRIAL_UHF) return AFQ_ERR_ARG;
-  if (d->precision != AFQ_FP64 && d->precision != AFQ_MIXED) return AFQ_ERR_ARG;
+  if (d->precision != AFQ_FP64 && d->precision != AFQ_MIXED && d->precision != AFQ_MIXED_HI)
+    return AFQ_ERR_ARG;
   if (d->n_exp_terms < 1 || d->n_exp_terms > 32) return AFQ_ERR_ARG;
   L.N = d->norb;
   L.G = d->nchol;
@@ -96,6 +133,19 @@ inline int make_layout(const afq_dims* d, Layout& L) {
     L.splitk = sk;
   }
   for (int s = 0; s < 2; ++s) L.ex[s] = choose_exch_tile(L.no[s], L.G, L.W);
+  L.mixed = d->precision != AFQ_FP64;
+  L.npc = d->precision == AFQ_MIXED_HI ? 3 : 2;
+  L.Kb = round8(L.Kfb_used);
+  L.Gb = round8(L.G);
+  L.Nb = round8(L.N);
+  L.Kv = round8(2LL * L.N);
+  for (int s = 0; s < 2; ++s) L.uex[s] = choose_uexch_tile(L.no[s], L.G, L.npc);
+  if (L.mixed) {  // the exchange partial sums follow the tensor-core tiling
+    for (int s = 0; s < L.ns; ++s) {
+      if (L.uex[s].bn == 0) return AFQ_ERR_SHAPE;  // no tile fits shared memory
+      L.ex[s].mt = L.uex[s].mt;
+    }
+  }
 
   // ---- prepared buffer
   long long o = 0;
@@ -124,6 +174,22 @@ inline int make_layout(const afq_dims* d, Layout& L) {
   for (int s = 0; s < L.np; ++s) L.p_exph1[s] = take((long long)L.N * L.Npad);
   L.p_mf = take(2LL * L.G);
   L.p_scal = take(8);
+  // bf16 operand pieces of the tensor-core path (n bf16 = n/4 doubles)
+  auto takeb = [&](long long nbf16, long long& ps) {
+    ps = align_up((nbf16 + 3) / 4, 32);
+    return take(ps * L.npc);
+  };
+  for (int s = 0; s < 2; ++s) L.q_exph1[s] = L.q_rc[s] = -1;
+  if (L.mixed) {
+    L.q_rccat = takeb((long long)L.G * L.Kb, L.q_rccat_ps);
+    L.q_cholT = takeb((long long)L.N * L.N * L.Gb, L.q_cholT_ps);
+    for (int s = 0; s < L.np; ++s) L.q_exph1[s] = takeb((long long)L.N * L.Nb, L.q_exph1_ps);
+    for (int s = 0; s < ntr; ++s) L.q_rc[s] = takeb((long long)L.G * L.no[s] * L.Nb, L.q_rc_ps[s]);
+    if (!L.uhf_trial) {
+      L.q_rc[1] = L.q_rc[0];
+      L.q_rc_ps[1] = L.q_rc_ps[0];
+    }
+  }
   L.prepared = o;
 
   // ---- workspace
@@ -149,6 +215,16 @@ inline int make_layout(const afq_dims* d, Layout& L) {
   L.w_cum = take(W);
   L.w_idx = take(W);  // int32 indices stored in double slots
   L.w_misc = take(64);
+  for (int s = 0; s < 2; ++s) L.v_gt[s] = -1;
+  if (L.mixed) {
+    L.v_gpl = takeb(2 * W * L.Kb, L.v_gpl_ps);
+    L.v_xt = takeb(2 * W * L.Gb, L.v_xt_ps);
+    L.v_vhs = takeb(W * N * L.Kv, L.v_vhs_ps);
+    L.v_bt[0] = takeb(W * 2 * L.nomax * L.Kv, L.v_bt_ps);
+    L.v_bt[1] = takeb(W * 2 * L.nomax * L.Kv, L.v_bt_ps);
+    L.v_acc = take((W * N * 2 * L.nomax + 1) / 2);  // fp32
+    for (int s = 0; s < L.ns; ++s) L.v_gt[s] = takeb(W * 2 * L.no[s] * L.Nb, L.v_gt_ps[s]);
+  }
   L.work = o;
   return AFQ_OK;
 }

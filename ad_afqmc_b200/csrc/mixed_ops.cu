@@ -1,0 +1,540 @@
+// Mixed-precision (tensor-core) contractions of the phaseless step.
+//
+// Each FP64 contraction of the step has a tcgen05 counterpart built on the
+// persistent split-BF16 GEMM (umma_gemm.cuh).  Operands are stored as two
+// (AFQ_MIXED) or three (AFQ_MIXED_HI) bf16 pieces; accumulation is FP32 in
+// TMEM.  Everything that decides walker survival stays FP64: Green's
+// functions, determinants, QR, weights and energy accumulation.
+//
+//   force bias   C (2W x G)  = Gpl (2W x K) . RCcat (G x K)^T, split over K
+//                (wavefunctions.py:1102-1126, 1314-1329)
+//   VHS          C (N^2 x 2W) = cholT (N^2 x G) . Xt (2W x G)^T
+//                written straight into the propagator's A operand pieces
+//                (propagation.py:196-203)
+//   propagator   per walker:  y = e^{-dt h/2} w ; t_n = VHS t_{n-1} / n ;
+//                w' = e^{-dt h/2} (y + sum t_n)   (propagation.py:154-176)
+//                iterates live as transposed bf16 pieces [t^T | (i t)^T] so
+//                that VHS (complex) times t is one real GEMM with K = 2N
+//   exchange     f = RC . Theta per (Cholesky vector, walker) tile, reduced
+//                in the epilogue to tr f and sum f o f^T; f never leaves the SM
+//                (wavefunctions.py:1128-1174, 1331-1363)
+#include <cuda.h>
+
+#include "afqmc_b200.h"
+#include "common.cuh"
+#include "ops.h"
+#include "profile.cuh"
+#include "umma_gemm.cuh"
+
+namespace afq {
+
+int make_tmap_bf16(CUtensorMap* map, const void* base, long long K, long long rows,
+                   long long batch, long long row_stride_elems, long long batch_stride_elems,
+                   int box_rows);
+int sm_count();
+
+namespace {
+
+__device__ __forceinline__ void named_sync_epi() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+inline int pairs_for(int npc, int* pa, int* pb) {
+  if (npc == 2) {
+    const int a[3] = {0, 0, 1}, b[3] = {0, 1, 0};
+    for (int i = 0; i < 3; ++i) { pa[i] = a[i]; pb[i] = b[i]; }
+    return 3;
+  }
+  const int a[6] = {0, 0, 1, 0, 1, 2}, b[6] = {0, 1, 0, 2, 1, 0};
+  for (int i = 0; i < 6; ++i) { pa[i] = a[i]; pb[i] = b[i]; }
+  return 6;
+}
+
+// ---------------------------------------------------------------------------
+// operand preparation
+// ---------------------------------------------------------------------------
+__global__ void split2d_kernel(const double* src, long long rows, long long cols, long long lds,
+                               int np, bf16* p0, bf16* p1, bf16* p2, long long ldd) {
+  bf16* P[3] = {p0, p1, p2};
+  const long long n = rows * cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / cols, c = e - r * cols;
+    put_pieces(src[r * lds + c], np, P, r * ldd + c);
+  }
+}
+
+// dst (C x R) = src (R x C)^T, split into pieces; 32x32 tiles through shared memory
+__global__ void transpose_split_kernel(const double* src, long long R, long long C, long long lds,
+                                       int np, bf16* p0, bf16* p1, bf16* p2, long long ldd) {
+  __shared__ double tile[32][33];
+  bf16* P[3] = {p0, p1, p2};
+  const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const long long r = r0 + i, c = c0 + threadIdx.x;
+    tile[i][threadIdx.x] = (r < R && c < C) ? src[r * lds + c] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const long long c = c0 + i, r = r0 + threadIdx.x;
+    if (c < C && r < R) put_pieces(tile[threadIdx.x][i], np, P, c * ldd + r);
+  }
+}
+
+// walker (W, N, nc) doubles -> pieces of its transpose (W, nc rows, K = N) with row stride ld
+__global__ void walker_t_kernel(const double* wk, int N, int nc, int np, bf16* p0, bf16* p1,
+                                bf16* p2, long long ld, long long bstride) {
+  __shared__ double tile[32][33];
+  bf16* P[3] = {p0, p1, p2};
+  const int b = blockIdx.z;
+  const int p0_ = blockIdx.x * 32, n0 = blockIdx.y * 32;
+  const double* src = wk + (long long)b * N * nc;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int p = p0_ + i, n = n0 + threadIdx.x;
+    tile[i][threadIdx.x] = (p < N && n < nc) ? src[(long long)p * nc + n] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int n = n0 + i, p = p0_ + threadIdx.x;
+    if (n < nc && p < N) put_pieces(tile[threadIdx.x][i], np, P, (long long)b * bstride + (long long)n * ld + p);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// epilogues
+// ---------------------------------------------------------------------------
+struct FbEpiU {
+  double* part;
+  long long ld, zstride;
+  template <int BN>
+  __device__ void tile(int z, int mti, int nti, int row, uint32_t taddr, const UmmaShape& s,
+                       uint8_t*) const {
+    const int m = mti * s.a_step + row;
+    double* dst = part + (long long)z * zstride + (long long)m * ld;
+#pragma unroll 1
+    for (int ch = 0; ch < BN / 16; ++ch) {
+      float v[16];
+      tmem_ld16(taddr + ch * 16, v);
+      if (m >= s.M) continue;
+      const int n0 = nti * s.b_step + ch * 16;
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        if (n0 + i < s.N) dst[n0 + i] = (double)v[i];
+    }
+  }
+};
+
+struct VhsEpiU {
+  bf16* vp[3];
+  int npc, N;
+  long long ld, wstride;
+  template <int BN>
+  __device__ void tile(int, int mti, int nti, int row, uint32_t taddr, const UmmaShape& s,
+                       uint8_t*) const {
+    const int q = mti * s.a_step + row;  // q = p*N + r
+    const int p = q / N, r = q - (q / N) * N;
+#pragma unroll 1
+    for (int ch = 0; ch < BN / 16; ++ch) {
+      float v[16];
+      tmem_ld16(taddr + ch * 16, v);
+      if (q >= s.M) continue;
+      const int n0 = nti * s.b_step + ch * 16;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int n = n0 + i;
+        if (n < s.N) {
+          const int w = n >> 1, c = n & 1;
+          put_pieces_f(v[i], npc, vp, (long long)w * wstride + (long long)p * ld + c * N + r);
+        }
+      }
+    }
+  }
+};
+
+enum { PM_Y = 0, PM_T = 1, PM_TLAST = 2, PM_OUT = 3 };
+
+struct PropEpiU {
+  int mode, npc, N, nc;
+  float scale;
+  float* acc;           // (W, N, nc) fp32
+  long long acc_bs;
+  bf16* bt[3];          // next B operand: (W, nc rows, ld) pieces
+  long long bt_ld, bt_bs;
+  double* wout;         // (W, N, nc) doubles
+  template <int BN>
+  __device__ void tile(int b, int mti, int, int row, uint32_t taddr, const UmmaShape& s,
+                       uint8_t*) const {
+    const int p = mti * s.a_step + row;
+    const bool ok = p < N;
+    float* arow = acc + (long long)b * acc_bs + (long long)p * nc;
+    const long long bbase = (long long)b * bt_bs;
+#pragma unroll 1
+    for (int ch = 0; ch < BN / 16; ++ch) {
+      float v[16];
+      tmem_ld16(taddr + ch * 16, v);
+      if (!ok) continue;
+      const int n0 = ch * 16;
+#pragma unroll
+      for (int i = 0; i < 16; i += 2) {
+        const int n = n0 + i;  // (re, im) pair of orbital j = n/2
+        if (n >= nc) break;
+        float tr = v[i], ti = v[i + 1];
+        if (mode == PM_OUT) {
+          double* o = wout + (long long)b * N * nc + (long long)p * nc + n;
+          o[0] = (double)tr;
+          o[1] = (double)ti;
+          continue;
+        }
+        if (mode != PM_Y) {
+          tr *= scale;
+          ti *= scale;
+        }
+        if (mode == PM_Y) {
+          arow[n] = tr;
+          arow[n + 1] = ti;
+        } else if (mode == PM_T) {
+          arow[n] += tr;
+          arow[n + 1] += ti;
+        } else {  // last term: hand the finished sum to the closing half-step
+          tr += arow[n];
+          ti += arow[n + 1];
+        }
+        // t^T rows n (re) and n+1 (im); columns [0,N): t, [N,2N): i*t
+        put_pieces_f(tr, npc, bt, bbase + (long long)n * bt_ld + p);
+        put_pieces_f(ti, npc, bt, bbase + (long long)(n + 1) * bt_ld + p);
+        if (mode != PM_TLAST) {
+          put_pieces_f(-ti, npc, bt, bbase + (long long)n * bt_ld + N + p);
+          put_pieces_f(tr, npc, bt, bbase + (long long)(n + 1) * bt_ld + N + p);
+        }
+      }
+    }
+  }
+};
+
+struct ExchEpiU {
+  int G, no, W, gpt, wpt;
+  double* cout;    // (W, G) complex
+  double* excout;  // (mt, W) complex
+  template <int BN>
+  __device__ void tile(int, int mti, int nti, int row, uint32_t taddr, const UmmaShape&,
+                       uint8_t* smem) const {
+    const int nc = 2 * no, fs = nc + 1;
+    float* Fs = reinterpret_cast<float*>(smem);
+    double4* pr = reinterpret_cast<double4*>(smem + ((128 * fs * 4 + 31) & ~31));
+    double2* ge = reinterpret_cast<double2*>(pr + 128);
+    const int g0 = mti * gpt, w0 = nti * wpt;
+    const int gcount = min(gpt, G - g0), wcount = min(wpt, W - w0);
+    const bool valid = row < gcount * no;
+    const int gl = row / no, i = row - (row / no) * no;
+    for (int wl = 0; wl < wcount; ++wl) {
+      const int cb = wl * nc;
+      const int c_lo = cb & ~15, c_hi = (cb + nc + 15) & ~15;
+      for (int c = c_lo; c < c_hi; c += 16) {
+        float v[16];
+        tmem_ld16(taddr + c, v);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int col = c + k - cb;
+          if (col >= 0 && col < nc) Fs[row * fs + col] = v[k];
+        }
+      }
+      named_sync_epi();
+      if (valid) {
+        double er = 0.0, ei = 0.0;
+        const float* fr = Fs + row * fs;
+        const float* fc = Fs + (gl * no) * fs + 2 * i;
+        for (int j = 0; j < no; ++j) {
+          const double ar = fr[2 * j], ai = fr[2 * j + 1];
+          const double br = fc[j * fs], bi = fc[j * fs + 1];
+          er += ar * br - ai * bi;
+          ei += ar * bi + ai * br;
+        }
+        pr[row] = make_double4(er, ei, (double)fr[2 * i], (double)fr[2 * i + 1]);
+      }
+      named_sync_epi();
+      if (row < gcount) {
+        double sr = 0, si = 0, tr = 0, ti = 0;
+        for (int ii = 0; ii < no; ++ii) {
+          const double4 q = pr[row * no + ii];
+          sr += q.x;
+          si += q.y;
+          tr += q.z;
+          ti += q.w;
+        }
+        const long long co = 2 * ((long long)(w0 + wl) * G + g0 + row);
+        cout[co] = tr;
+        cout[co + 1] = ti;
+        ge[row] = make_double2(sr, si);
+      }
+      named_sync_epi();
+      if (row == 0) {
+        double sx = 0, sy = 0;
+        for (int g = 0; g < gcount; ++g) {
+          sx += ge[g].x;
+          sy += ge[g].y;
+        }
+        excout[2 * ((long long)mti * W + w0 + wl)] = sx;
+        excout[2 * ((long long)mti * W + w0 + wl) + 1] = sy;
+      }
+    }
+  }
+  static size_t smem_extra(int no) {
+    const int fs = 2 * no + 1;
+    return ((size_t(128) * fs * 4 + 31) & ~size_t(31)) + 128 * sizeof(double4) + 128 * sizeof(double2);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+template <class Epi>
+int setup_maps(UmmaParams<Epi>& P, bf16* const a[3], int npa, long long aK, long long arows,
+               long long abatch, long long ald, long long abs, bf16* const b[3], int npb,
+               long long bK, long long brows, long long bbatch, long long bld, long long bbs,
+               int bn) {
+  for (int i = 0; i < npa; ++i) {
+    int rc = make_tmap_bf16(&P.ta[i], a[i], aK, arows, abatch, ald, abs, kUBM);
+    if (rc != AFQ_OK) return rc;
+  }
+  for (int j = 0; j < npb; ++j) {
+    int rc = make_tmap_bf16(&P.tb[j], b[j], bK, brows, bbatch, bld, bbs, bn);
+    if (rc != AFQ_OK) return rc;
+  }
+  return AFQ_OK;
+}
+
+template <class Epi>
+void base_shape(UmmaParams<Epi>& P, int npc, int M, int N, int K, int batch, int bn, int* err) {
+  P.s.npa = P.s.npb = npc;
+  P.s.npairs = pairs_for(npc, P.s.pa, P.s.pb);
+  P.s.M = M;
+  P.s.N = N;
+  P.s.K = K;
+  P.s.batch = batch;
+  P.s.a_batched = 1;
+  P.s.a_step = kUBM;
+  P.s.b_step = bn;
+  P.s.mt = (M + kUBM - 1) / kUBM;
+  P.s.nt = (N + bn - 1) / bn;
+  P.s.ksplit = 1;
+  P.s.kchunk = (K + kUBK - 1) / kUBK * kUBK;
+  P.s.err = err;
+}
+
+template <int BN, class Epi>
+int run(UmmaParams<Epi>& P, size_t extra, cudaStream_t st, int prof_id) {
+  P.s.stages = umma_pick_stages(BN, P.s.npa, P.s.npb, extra);
+  if (P.s.stages < 2) return AFQ_ERR_SHAPE;
+  ProfScope ps(prof_id, st);
+  return launch_umma<BN>(P, extra, sm_count(), st) == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
+}
+
+int* err_flag(const Layout& L, double* work) {
+  return reinterpret_cast<int*>(work + L.w_misc);
+}
+
+template <int BN>
+int prop_launch(const Layout& L, const double* prep, double* work, int s, int nc, int mode,
+                float scale, bf16* const a[3], long long aK, long long ald, long long abs,
+                int a_batched, bf16* const bsrc[3], bf16* const bdst[3], double* wout,
+                cudaStream_t st) {
+  UmmaParams<PropEpiU> P{};
+  const int N = L.N;
+  const long long btbs = 2LL * L.nomax * L.Kv;
+  int rc = setup_maps(P, a, L.npc, aK, N, a_batched ? L.W : 1, ald, abs, bsrc, L.npc, aK, nc, L.W,
+                      L.Kv, btbs, BN);
+  if (rc != AFQ_OK) return rc;
+  base_shape(P, L.npc, N, nc, (int)aK, L.W, BN, err_flag(L, work));
+  P.s.a_batched = a_batched;
+  P.epi.mode = mode;
+  P.epi.npc = L.npc;
+  P.epi.N = N;
+  P.epi.nc = nc;
+  P.epi.scale = scale;
+  P.epi.acc = reinterpret_cast<float*>(work + L.v_acc);
+  P.epi.acc_bs = (long long)N * nc;
+  for (int i = 0; i < 3; ++i) P.epi.bt[i] = bdst ? bdst[i] : nullptr;
+  P.epi.bt_ld = L.Kv;
+  P.epi.bt_bs = btbs;
+  P.epi.wout = wout;
+  return run<BN>(P, 0, st, K_PROP);
+}
+
+template <int BN>
+int exch_launch(const Layout& L, const double* prep, double* work, int s, cudaStream_t st) {
+  const UExchTile& X = L.uex[s];
+  const int no = L.no[s];
+  UmmaParams<ExchEpiU> P{};
+  bf16* a[3];
+  bf16* b[3];
+  piece_ptrs(const_cast<double*>(prep), L.q_rc[s], L.q_rc_ps[s], L.npc, a);
+  piece_ptrs(work, L.v_gt[s], L.v_gt_ps[s], L.npc, b);
+  const long long arows = (long long)L.G * no, brows = (long long)L.W * 2 * no;
+  int rc = setup_maps(P, a, L.npc, L.N, arows, 1, L.Nb, arows * L.Nb, b, L.npc, L.N, brows, 1,
+                      L.Nb, brows * L.Nb, BN);
+  if (rc != AFQ_OK) return rc;
+  base_shape(P, L.npc, (int)arows, (int)brows, L.N, 1, BN, err_flag(L, work));
+  P.s.a_step = X.gpt * no;
+  P.s.b_step = X.wpt * 2 * no;
+  P.s.mt = X.mt;
+  P.s.nt = (L.W + X.wpt - 1) / X.wpt;
+  P.epi.G = L.G;
+  P.epi.no = no;
+  P.epi.W = L.W;
+  P.epi.gpt = X.gpt;
+  P.epi.wpt = X.wpt;
+  P.epi.cout = work + L.w_c[s];
+  P.epi.excout = work + L.w_exc[s];
+  return run<BN>(P, ExchEpiU::smem_extra(no), st, K_EXCH);
+}
+
+}  // namespace
+
+int mixed_prepare(const Layout& L, double* P, cudaStream_t st) {
+  ProfScope ps(K_MISC, st);
+  bf16* q[3];
+  // force-bias operand: rot_chol concatenated over spins (G x Kfb)
+  piece_ptrs(P, L.q_rccat, L.q_rccat_ps, L.npc, q);
+  split2d_kernel<<<1184, 256, 0, st>>>(P + L.p_rccat, L.G, L.Kfb_used, L.Kfb, L.npc, q[0], q[1],
+                                       q[2], L.Kb);
+  // VHS operand: chol transposed to (N^2 x G)
+  piece_ptrs(P, L.q_cholT, L.q_cholT_ps, L.npc, q);
+  {
+    const long long NN = (long long)L.N * L.N;
+    dim3 grid((unsigned)((NN + 31) / 32), (unsigned)((L.G + 31) / 32));
+    transpose_split_kernel<<<grid, dim3(32, 8), 0, st>>>(P + L.p_chol, L.G, NN, L.N2pad, L.npc,
+                                                         q[0], q[1], q[2], L.Gb);
+  }
+  for (int s = 0; s < L.np; ++s) {
+    piece_ptrs(P, L.q_exph1[s], L.q_exph1_ps, L.npc, q);
+    split2d_kernel<<<296, 256, 0, st>>>(P + L.p_exph1[s], L.N, L.N, L.Npad, L.npc, q[0], q[1],
+                                        q[2], L.Nb);
+  }
+  const int ntr = L.uhf_trial ? 2 : 1;
+  for (int s = 0; s < ntr; ++s) {
+    piece_ptrs(P, L.q_rc[s], L.q_rc_ps[s], L.npc, q);
+    split2d_kernel<<<1184, 256, 0, st>>>(P + L.p_rc[s], (long long)L.G * L.no[s], L.N, L.Npad,
+                                         L.npc, q[0], q[1], q[2], L.Nb);
+  }
+  return cudaGetLastError() == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
+}
+
+int mixed_fb_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {
+  constexpr int BN = 128;
+  UmmaParams<FbEpiU> P{};
+  bf16* a[3];
+  bf16* b[3];
+  piece_ptrs(work, L.v_gpl, L.v_gpl_ps, L.npc, a);
+  piece_ptrs(const_cast<double*>(prep), L.q_rccat, L.q_rccat_ps, L.npc, b);
+  const long long K = L.Kfb_used, M = 2LL * L.W;
+  int rc = setup_maps(P, a, L.npc, K, M, 1, L.Kb, M * L.Kb, b, L.npc, K, L.G, 1, L.Kb,
+                      (long long)L.G * L.Kb, BN);
+  if (rc != AFQ_OK) return rc;
+  base_shape(P, L.npc, (int)M, L.G, (int)K, 1, BN, err_flag(L, work));
+  const long long kblocks = (K + kUBK - 1) / kUBK;
+  const long long per = (kblocks + L.splitk - 1) / L.splitk;
+  P.s.ksplit = L.splitk;
+  P.s.kchunk = (int)(per * kUBK);
+  P.epi.part = work + L.w_fbpart;
+  P.epi.ld = L.Gpad;
+  P.epi.zstride = 2LL * L.W * L.Gpad;
+  return run<BN>(P, 0, st, K_FB);
+}
+
+int mixed_vhs_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {
+  constexpr int BN = 256;
+  UmmaParams<VhsEpiU> P{};
+  bf16* a[3];
+  bf16* b[3];
+  piece_ptrs(const_cast<double*>(prep), L.q_cholT, L.q_cholT_ps, L.npc, a);
+  piece_ptrs(work, L.v_xt, L.v_xt_ps, L.npc, b);
+  const long long NN = (long long)L.N * L.N, M2 = 2LL * L.W;
+  int rc = setup_maps(P, a, L.npc, L.G, NN, 1, L.Gb, NN * L.Gb, b, L.npc, L.G, M2, 1, L.Gb,
+                      M2 * L.Gb, BN);
+  if (rc != AFQ_OK) return rc;
+  base_shape(P, L.npc, (int)NN, (int)M2, L.G, 1, BN, err_flag(L, work));
+  piece_ptrs(work, L.v_vhs, L.v_vhs_ps, L.npc, P.epi.vp);
+  P.epi.npc = L.npc;
+  P.epi.N = L.N;
+  P.epi.ld = L.Kv;
+  P.epi.wstride = (long long)L.N * L.Kv;
+  return run<BN>(P, 0, st, K_VHS);
+}
+
+template <int BN>
+static int propagate_one(const Layout& L, const double* prep, double* work, double* wk, int s,
+                         int n_exp_terms, cudaStream_t st) {
+  const int N = L.N, nc = 2 * L.no[s];
+  bf16 *e[3], *v[3], *b0[3], *b1[3];
+  piece_ptrs(const_cast<double*>(prep), L.q_exph1[s], L.q_exph1_ps, L.npc, e);
+  piece_ptrs(work, L.v_vhs, L.v_vhs_ps, L.npc, v);
+  piece_ptrs(work, L.v_bt[0], L.v_bt_ps, L.npc, b0);
+  piece_ptrs(work, L.v_bt[1], L.v_bt_ps, L.npc, b1);
+  const long long btbs = 2LL * L.nomax * L.Kv;
+  {
+    ProfScope ps(K_MISC, st);
+    dim3 grid((N + 31) / 32, (nc + 31) / 32, L.W);
+    walker_t_kernel<<<grid, dim3(32, 8), 0, st>>>(wk, N, nc, L.npc, b0[0], b0[1], b0[2], L.Kv,
+                                                  btbs);
+    if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+  }
+  const long long vbs = (long long)N * L.Kv;
+  if (n_exp_terms <= 1) {
+    int rc = prop_launch<BN>(L, prep, work, s, nc, PM_Y, 1.f, e, N, L.Nb, N * L.Nb, 0, b0, b1,
+                             nullptr, st);
+    if (rc != AFQ_OK) return rc;
+    return prop_launch<BN>(L, prep, work, s, nc, PM_OUT, 1.f, e, N, L.Nb, N * L.Nb, 0, b1, nullptr,
+                           wk, st);
+  }
+  // y = e^{-dt h/2} w  -> acc, and [y^T | (i y)^T] into b1
+  int rc = prop_launch<BN>(L, prep, work, s, nc, PM_Y, 1.f, e, N, L.Nb, N * L.Nb, 0, b0, b1,
+                           nullptr, st);
+  if (rc != AFQ_OK) return rc;
+  bf16** src = b1;
+  bf16** dst = b0;
+  for (int n = 1; n < n_exp_terms; ++n) {
+    const int mode = (n == n_exp_terms - 1) ? PM_TLAST : PM_T;
+    rc = prop_launch<BN>(L, prep, work, s, nc, mode, 1.f / n, v, 2LL * N, L.Kv, vbs, 1, src, dst,
+                         nullptr, st);
+    if (rc != AFQ_OK) return rc;
+    bf16** t = src;
+    src = dst;
+    dst = t;
+  }
+  // w' = e^{-dt h/2} (y + sum t_n): B operand holds the finished sum
+  return prop_launch<BN>(L, prep, work, s, nc, PM_OUT, 1.f, e, N, L.Nb, N * L.Nb, 0, src, nullptr,
+                         wk, st);
+}
+
+int mixed_propagate_walkers(const Layout& L, const double* prep, double* work,
+                            double* const walkers[2], int n_exp_terms, cudaStream_t st) {
+  for (int s = 0; s < L.np; ++s) {
+    const int nc = 2 * L.no[s];
+    int rc;
+    if (nc <= 16)
+      rc = propagate_one<16>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (nc <= 32)
+      rc = propagate_one<32>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (nc <= 48)
+      rc = propagate_one<48>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (nc <= 64)
+      rc = propagate_one<64>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (nc <= 80)
+      rc = propagate_one<80>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (nc <= 96)
+      rc = propagate_one<96>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else
+      rc = propagate_one<128>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    if (rc != AFQ_OK) return rc;
+  }
+  return AFQ_OK;
+}
+
+int mixed_exchange(const Layout& L, const double* prep, double* work, int s, cudaStream_t st) {
+  switch (L.uex[s].bn) {
+    case 240: return exch_launch<240>(L, prep, work, s, st);
+    case 160: return exch_launch<160>(L, prep, work, s, st);
+    case 128: return exch_launch<128>(L, prep, work, s, st);
+    default: return exch_launch<80>(L, prep, work, s, st);
+  }
+}
+
+}  // namespace afq

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include "common.cuh"
 #include "layout.cuh"
 
 namespace afq {
@@ -16,6 +17,8 @@ struct GreenSector {
   long long koff;       // offset of this sector inside a G-planar row
   double* theta;        // (W, N, no) complex or nullptr
   double* gout;         // (W, no, N) complex or nullptr
+  bf16* gtb[3];         // exchange operand pieces: rows (w, j, re/im), row stride ldtb, or nullptr
+  long long ldtb;
 };
 struct GreenArgs {
   int N, W, ns;
@@ -23,6 +26,9 @@ struct GreenArgs {
   double* wscal;        // per-walker scalars (16 doubles) or nullptr
   double* gpl;          // (2W, ldg) planar G or nullptr
   long long ldg;
+  int npc;              // bf16 pieces for the *b outputs
+  bf16* gplb[3];        // force-bias operand pieces (2W, ldgb) or nullptr
+  long long ldgb;
 };
 cudaError_t launch_green(const GreenArgs& a, cudaStream_t st);
 // overlaps from per-sector determinants in wscal: out[w] = det0^mult (or det0*det1)
@@ -62,5 +68,19 @@ cudaError_t launch_normal(double* out, long long n, unsigned long long seed,
                           unsigned long long offset, cudaStream_t st);
 cudaError_t launch_set_scalars(double* dst, double a, double b, double c, double d,
                                cudaStream_t st);
+
+// ---- tensor-core (mixed precision) path (mixed_ops.cu) ---------------------
+int mixed_prepare(const Layout& L, double* prepared, cudaStream_t st);
+int mixed_fb_gemm(const Layout& L, const double* prepared, double* work, cudaStream_t st);
+int mixed_vhs_gemm(const Layout& L, const double* prepared, double* work, cudaStream_t st);
+int mixed_propagate_walkers(const Layout& L, const double* prepared, double* work,
+                            double* const walkers[2], int n_exp_terms, cudaStream_t st);
+int mixed_exchange(const Layout& L, const double* prepared, double* work, int sector,
+                   cudaStream_t st);
+// bf16 piece pointers of a buffer at offset `off` (doubles) with piece stride `ps`
+inline void piece_ptrs(double* base, long long off, long long ps, int npc, bf16* out[3]) {
+  for (int i = 0; i < 3; ++i)
+    out[i] = i < npc ? reinterpret_cast<bf16*>(base + off + i * ps) : nullptr;
+}
 
 }  // namespace afq

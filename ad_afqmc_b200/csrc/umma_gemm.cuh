@@ -1,0 +1,231 @@
+// Persistent tcgen05 GEMM with split-BF16 operands (sm_100a).
+//
+//   C[b] (M x N, fp32 in TMEM) = sum_{p in pairs} A_{pa[p]}[b] (M x K) * B_{pb[p]}[b]^T (N x K)
+//
+// A value x is stored as bf16 pieces x = x_0 + x_1 (+ x_2); the pair list
+// {(0,0),(0,1),(1,0)} is the "BF16x3" product (about 16 significant bits),
+// {(0,0),(0,1),(1,0),(0,2),(1,1),(2,0)} with three pieces about 24 bits.
+//
+// Roles (192 threads, one CTA per SM, persistent over tiles):
+//   warp 0      TMA producer: 128-byte-swizzled K-major tiles into a STAGES ring
+//   warp 1      TMEM allocator; lane 0 issues tcgen05.mma into one of two
+//               accumulators and commits stage/accumulator barriers
+//   warps 2..5  epilogue: tcgen05.ld rows of the finished accumulator (one TMEM
+//               lane per thread) and hand 32 columns at a time to the functor
+// All waits are bounded; on timeout the CTA records an error and unwinds.
+#pragma once
+
+#include "common.cuh"
+#include "umma.cuh"
+
+namespace afq {
+
+constexpr int kUBM = 128;  // UMMA M
+constexpr int kUBK = 64;   // K per stage (128 bytes of bf16: one swizzle row)
+
+struct UmmaShape {
+  int stages;        // depth of the shared-memory ring (host-chosen)
+  int a_batched;     // 0: A is shared by every batch (tensor map batch extent 1)
+  int M, N, K;       // per batch
+  int batch;
+  int mt, nt;        // tiles along M and N
+  int a_step, b_step;  // rows of A / B advanced per tile (<= 128 / BN)
+  int ksplit, kchunk;  // K split into ksplit chunks of kchunk (multiple of 64)
+  int npa, npb;      // pieces of A and B
+  int npairs;
+  int pa[6], pb[6];
+  int* err;          // device error flag (set to 1 on a timed-out wait)
+};
+
+template <class Epi>
+struct UmmaParams {
+  CUtensorMap ta[3];
+  CUtensorMap tb[3];
+  UmmaShape s;
+  Epi epi;
+};
+
+__host__ __device__ constexpr int umma_tmem_cols(int bn) {
+  int c = 32;
+  while (c < 2 * bn) c <<= 1;
+  return c;
+}
+
+constexpr size_t kUmmaSmemBudget = 227 * 1024;
+
+__host__ __device__ inline size_t umma_stage_bytes(int bn, int npa, int npb) {
+  return size_t(npa) * kUBM * 128 + size_t(npb) * bn * 128;
+}
+__host__ __device__ inline size_t umma_smem_bytes(int bn, int stages, int npa, int npb,
+                                                  size_t extra) {
+  return 1024 /*alignment slack*/ + size_t(stages) * umma_stage_bytes(bn, npa, npb) +
+         256 /*barriers*/ + extra;
+}
+// deepest ring (<= 8) that fits next to `extra` bytes of epilogue scratch
+inline int umma_pick_stages(int bn, int npa, int npb, size_t extra) {
+  for (int st = 8; st >= 2; --st)
+    if (umma_smem_bytes(bn, st, npa, npb, extra) <= kUmmaSmemBudget) return st;
+  return 0;
+}
+
+template <int BN, class Epi>
+__global__ void __launch_bounds__(192, 1) umma_gemm_kernel(const __grid_constant__ UmmaParams<Epi> P) {
+  static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M=128");
+  static_assert(umma_tmem_cols(BN) <= 512, "two accumulators must fit in TMEM");
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const UmmaShape& S = P.s;
+  const int ST = S.stages;
+  const uint32_t a_bytes = kUBM * 128, b_bytes = BN * 128;
+  const uint32_t stage_bytes = S.npa * a_bytes + S.npb * b_bytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * stage_bytes);
+  uint64_t* empty = full + ST;
+  uint64_t* accf = empty + ST;
+  uint64_t* acce = accf + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce + 2);
+  volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  uint8_t* epi_smem = reinterpret_cast<uint8_t*>(full) + 256;  // epilogue scratch
+  constexpr uint32_t kCols = umma_tmem_cols(BN);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
+    *abort_s = 0;
+    fence_barrier_init();
+  }
+  if (warp == 0 && lane == 0) {
+    for (int i = 0; i < S.npa; ++i) prefetch_tmap(&P.ta[i]);
+    for (int i = 0; i < S.npb; ++i) prefetch_tmap(&P.tb[i]);
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, kCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+
+  const int tiles = S.batch * S.ksplit * S.mt * S.nt;
+  auto fail = [&]() {
+    atomicExch(S.err, 1);
+    *abort_s = 1;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      for (int tile = blockIdx.x; tile < tiles && !*abort_s; tile += gridDim.x) {
+        const int nti = tile % S.nt, rest = tile / S.nt;
+        const int mti = rest % S.mt, z = rest / S.mt;
+        const int b = z / S.ksplit, k0 = (z % S.ksplit) * S.kchunk;
+        const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
+        for (int kb = 0; kb < KB; ++kb) {
+          if (!mbar_wait(&empty[stage], phase ^ 1)) { fail(); break; }
+          mbar_arrive_expect_tx(&full[stage], stage_bytes);
+          uint8_t* sa = smem + stage * stage_bytes;
+          uint8_t* sb = sa + S.npa * a_bytes;
+          for (int i = 0; i < S.npa; ++i)
+            tma_load_3d(sa + i * a_bytes, &P.ta[i], &full[stage], k0 + kb * kUBK,
+                        mti * S.a_step, S.a_batched ? b : 0);
+          for (int j = 0; j < S.npb; ++j)
+            tma_load_3d(sb + j * b_bytes, &P.tb[j], &full[stage], k0 + kb * kUBK, nti * S.b_step,
+                        b);
+          if (++stage == ST) { stage = 0; phase ^= 1; }
+        }
+      }
+      // drain: wait (bounded) until the MMA side released every stage we filled
+      for (int s = 0; s < ST; ++s) {
+        if (!mbar_wait(&empty[stage], phase ^ 1)) { fail(); break; }
+        if (++stage == ST) { stage = 0; phase ^= 1; }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = instr_desc(kUBM, BN, 1);
+      int stage = 0;
+      uint32_t phase = 0;
+      int it = 0;
+      for (int tile = blockIdx.x; tile < tiles && !*abort_s; tile += gridDim.x, ++it) {
+        const int buf = it & 1;
+        const uint32_t use = (uint32_t)(it >> 1);
+        if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); break; }
+        tc_fence_after();
+        const uint32_t dt = tbase + buf * BN;
+        const int k0 = ((tile / (S.nt * S.mt)) % S.ksplit) * S.kchunk;
+        const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
+        bool ok = true;
+        for (int kb = 0; kb < KB; ++kb) {
+          if (!mbar_wait(&full[stage], phase)) { fail(); ok = false; break; }
+          tc_fence_after();
+          const uint8_t* sa = smem + stage * stage_bytes;
+          const uint8_t* sb = sa + S.npa * a_bytes;
+          for (int p = 0; p < S.npairs; ++p) {
+            const uint64_t ad = smem_desc_sw128(sa + S.pa[p] * a_bytes);
+            const uint64_t bd = smem_desc_sw128(sb + S.pb[p] * b_bytes);
+#pragma unroll
+            for (int ks = 0; ks < kUBK / 16; ++ks)
+              umma_bf16(dt, ad + 2 * ks, bd + 2 * ks, idesc, (kb | p | ks) != 0);
+          }
+          umma_commit(&empty[stage]);
+          if (++stage == ST) { stage = 0; phase ^= 1; }
+        }
+        if (!ok) break;
+        umma_commit(&accf[buf]);
+      }
+    }
+  } else {
+    const int sub = warp & 3;
+    const int row = sub * 32 + lane;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
+      const int buf = it & 1;
+      const uint32_t use = (uint32_t)(it >> 1);
+      if (!mbar_wait_abortable(&accf[buf], use & 1, abort_s)) { fail(); break; }
+      tc_fence_after();
+      const int nti = tile % S.nt, rest = tile / S.nt;
+      const int mti = rest % S.mt, z = rest / S.mt;
+      // z = batch * ksplit + split
+      P.epi.template tile<BN>(z, mti, nti, row, tbase + ((uint32_t)(sub * 32) << 16) + buf * BN, S,
+                              epi_smem);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[buf]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tbase, kCols);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side: tensor maps and launch
+// ---------------------------------------------------------------------------
+// 3-D bf16 tensor map: dims {K, rows, batch}; box {64, box_rows, 1}; SW128.
+int make_tmap_bf16(CUtensorMap* map, const void* base, long long K, long long rows,
+                   long long batch, long long row_stride_elems, long long batch_stride_elems,
+                   int box_rows);
+
+// P.s.stages must come from umma_pick_stages(BN, npa, npb, epi_extra).
+template <int BN, class Epi>
+cudaError_t launch_umma(const UmmaParams<Epi>& P, size_t epi_extra, int num_sms, cudaStream_t st) {
+  const size_t smem = umma_smem_bytes(BN, P.s.stages, P.s.npa, P.s.npb, epi_extra);
+  if (P.s.stages < 2 || smem > kUmmaSmemBudget) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(umma_gemm_kernel<BN, Epi>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int tiles = P.s.batch * P.s.ksplit * P.s.mt * P.s.nt;
+  const int grid = tiles < num_sms ? tiles : num_sms;
+  umma_gemm_kernel<BN, Epi><<<grid, 192, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+}  // namespace afq

@@ -46,7 +46,12 @@ typedef enum afq_status {
 
 enum { AFQ_RESTRICTED = 0, AFQ_UNRESTRICTED = 1 };      /* walker_type  */
 enum { AFQ_TRIAL_RHF = 0, AFQ_TRIAL_UHF = 1 };          /* trial_type   */
-enum { AFQ_FP64 = 0, AFQ_MIXED = 1 };                   /* precision    */
+/* precision: AFQ_FP64 everywhere; AFQ_MIXED: force bias, VHS, propagator
+ * and exchange contractions on tcgen05 tensor cores with operands split into
+ * two bfloat16 pieces (three products, FP32 accumulation); AFQ_MIXED_HI: three
+ * pieces, six products.  Green's functions, determinants, QR, weights and
+ * energy accumulation stay FP64 in every mode. */
+enum { AFQ_FP64 = 0, AFQ_MIXED = 1, AFQ_MIXED_HI = 2 };
 enum { AFQ_SR_LOCAL = 0, AFQ_SR_GLOBAL = 1 };           /* sr z-formula */
 
 /* Problem sizes and method switches (fixed for one prepared buffer). */
@@ -172,6 +177,25 @@ int afq_block_end(const afq_dims* d, const void* prepared, afq_state* s, double*
  * Replaces random.normal(subkey, (S, W, G)) in sampler._block_scan
  * (sampling.py:63-71); the bits differ from JAX threefry by design. */
 int afq_normal_fields(double* out, int64_t n, uint64_t seed, uint64_t offset, void* stream);
+
+/* Split x (n,) float64 into npieces (1..3) bfloat16 arrays with
+ * x ~= p0 + p1 (+ p2), each piece rounded to nearest from the remainder.
+ * Operand preparation of the mixed-precision contractions; no counterpart in
+ * the reference (which uses float32/complex64 there, launch_script.py:654-657). */
+int afq_split_bf16(const double* x, int64_t n, int npieces, void* const pieces[3], void* stream);
+
+/* C[b] (M x N, float32, row stride ldc) = sum over pairs (i,j) of
+ * A_i[b] (M x K) * B_j[b]^T (N x K), all pieces bfloat16 K-contiguous with row
+ * strides lda/ldb (multiples of 8 elements) and batch strides (0 = packed).
+ * pairs: npairs (i,j) index pairs.  tcgen05 tensor cores, FP32 accumulation.
+ * err_flag: device int set to 1 if an internal wait timed out.
+ * The split-operand GEMM behind the mixed-precision force bias, VHS and
+ * exchange contractions (the reference's vhs_mixed_precision switch,
+ * propagation.py:196-203); exposed for direct use and testing. */
+int afq_gemm_split_bf16(const void* const a_pieces[3], int npa, const void* const b_pieces[3],
+                        int npb, int npairs, const int32_t* pairs, int M, int N, int K, int batch,
+                        int64_t lda, int64_t a_bstride, int64_t ldb, int64_t b_bstride, float* C,
+                        int64_t ldc, int64_t c_bstride, int32_t* err_flag, void* stream);
 
 /* Instrumentation (no counterpart in the reference, which has no native
  * code): launches of one kernel family (kernel_id >= 0) or of all library

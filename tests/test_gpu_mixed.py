@@ -1,0 +1,123 @@
+"""Mixed-precision (tcgen05, split-BF16) walker path against FP64.
+
+Tolerances are the measured accuracy of the two-piece (BF16x3) and
+three-piece (BF16x6) products with FP32 accumulation; every quantity that
+decides walker survival (Green's functions, determinants, QR, weights) is
+FP64 in both modes, so the differences come only from the contractions.
+"""
+
+import copy
+
+import numpy as np
+import pytest
+import torch
+
+from ad_afqmc_b200.synthetic import make_system
+from oracle import afqmc_oracle as orc
+from tests._helpers import ListSource, device_system, near_trial_walkers, oracle_system, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _walkers(sys_, W, seed, wt):
+    rng = np.random.default_rng(seed)
+    if wt == "restricted":
+        mo = sys_.mo_coeff if sys_.trial == "rhf" else sys_.mo_coeff[0]
+        return near_trial_walkers(rng, mo, W, eps=0.1)
+    mo = sys_.mo_coeff if sys_.trial == "uhf" else [sys_.mo_coeff, sys_.mo_coeff]
+    return [near_trial_walkers(rng, mo[0], W, eps=0.1), near_trial_walkers(rng, mo[1], W, eps=0.1)]
+
+
+def _dev(w):
+    from ad_afqmc_b200.walkers import RHFWalkers, UHFWalkers
+
+    return UHFWalkers([w[0].copy(), w[1].copy()]) if isinstance(w, list) else RHFWalkers(w.copy())
+
+
+CASES = [
+    (24, (6, 6), 96, "rhf", "restricted", 16),
+    (64, (16, 16), 300, "rhf", "restricted", 40),
+    (48, (13, 11), 200, "uhf", "unrestricted", 24),
+    (200, (40, 40), 1000, "rhf", "restricted", 8),
+]
+TOL = {"mixed": 1e-4, "mixed_hi": 5e-6}
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_hi"])
+@pytest.mark.parametrize("case", CASES)
+def test_mixed_measurements(case, precision):
+    norb, nelec, nchol, tr, wt, W = case
+    sys_ = make_system(norb, nelec, nchol, seed=11, trial=tr, chol_scale=0.25)
+    walkers = _walkers(sys_, W, 3, wt)
+    o_trial, o_ham, o_wave, _ = oracle_system(sys_, wt, 0.005)
+    d_trial, d_ham, d_wave, d_prop, _ = device_system(sys_, wt, 0.005, W, precision=precision)
+    eng = d_prop.engine(d_ham, d_trial, d_wave)
+    # measurements through the engine of the requested precision
+    import ctypes as C
+    from ad_afqmc_b200 import _lib
+    from ad_afqmc_b200.wavefunctions import _ptrs
+    dw = _dev(walkers)
+    fb = torch.empty(W, nchol, dtype=torch.complex128, device="cuda")
+    p, w, wb = eng.handle
+    _lib.check(_lib.lib().afq_calc_force_bias(C.byref(eng.dims), p, _ptrs(dw), fb.data_ptr(), w, wb,
+                                              _lib.stream_handle()), "fb")
+    e = torch.empty(W, dtype=torch.complex128, device="cuda")
+    _lib.check(_lib.lib().afq_calc_energy(C.byref(eng.dims), p, _ptrs(dw), e.data_ptr(), w, wb,
+                                          _lib.stream_handle()), "energy")
+    fb_o = o_trial.calc_force_bias(walkers, o_ham, o_wave)
+    e_o = o_trial.calc_energy(walkers, o_ham, o_wave)
+    assert rel_err(_np(fb), fb_o) < TOL[precision]
+    err_e = np.max(np.abs(_np(e) - e_o))
+    scale = np.max(np.abs(e_o))
+    assert err_e / scale < TOL[precision], (err_e, scale)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_hi"])
+@pytest.mark.parametrize("case", CASES[:3])
+def test_mixed_step(case, precision):
+    norb, nelec, nchol, tr, wt, W = case
+    sys_ = make_system(norb, nelec, nchol, seed=12, trial=tr, chol_scale=0.25)
+    walkers = _walkers(sys_, W, 4, wt)
+    rng = np.random.default_rng(5)
+    fields = rng.standard_normal((W, nchol))
+    o_trial, o_ham, o_wave, o_prop = oracle_system(sys_, wt, 0.005)
+    o_prop.n_walkers = W
+    o_pd = o_prop.init_prop_data(o_trial, o_wave, o_ham, init_walkers=copy.deepcopy(walkers))
+    o_pd = o_prop.propagate_constrained(o_trial, o_ham, o_pd, fields, o_wave)
+    d_trial, d_ham, d_wave, d_prop, _ = device_system(sys_, wt, 0.005, W, precision=precision)
+    d_pd = d_prop.init_prop_data(d_trial, d_wave, d_ham, 0, init_walkers=_dev(walkers))
+    d_pd = d_prop.propagate_constrained(d_trial, d_ham, d_pd, fields, d_wave)
+    if wt == "restricted":
+        pairs = [(_np(d_pd["walkers"].data), o_pd["walkers"])]
+    else:
+        pairs = [(_np(d_pd["walkers"].data[s]), o_pd["walkers"][s]) for s in range(2)]
+    for d, o in pairs:
+        assert rel_err(d, o) < TOL[precision]
+    assert np.allclose(_np(d_pd["weights"]), o_pd["weights"], rtol=10 * TOL[precision], atol=1e-6)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_hi"])
+def test_mixed_block_energy_error(precision):
+    """Block energies of the mixed path vs the FP64 oracle (same fields)."""
+    from ad_afqmc_b200 import sampling
+
+    sys_ = make_system(64, (16, 16), 300, seed=13, trial="rhf", chol_scale=0.25)
+    W, S, nb = 32, 5, 3
+    walkers = _walkers(sys_, W, 6, "restricted")
+    rng = np.random.default_rng(7)
+    fields = [rng.standard_normal((S, W, 300)) for _ in range(nb)]
+    uni = list(rng.random(nb))
+    o_trial, o_ham, o_wave, o_prop = oracle_system(sys_, "restricted", 0.005)
+    o_prop.n_walkers = W
+    o_pd = o_prop.init_prop_data(o_trial, o_wave, o_ham, init_walkers=copy.deepcopy(walkers))
+    e_o, o_pd = orc.Sampler(S, nb, 1).propagate_phaseless(o_prop, o_trial, o_ham, o_pd, o_wave,
+                                                          ListSource(fields, uni))
+    d_trial, d_ham, d_wave, d_prop, ham = device_system(sys_, "restricted", 0.005, W, precision=precision)
+    d_pd = d_prop.init_prop_data(d_trial, d_wave, d_ham, 0, init_walkers=_dev(walkers))
+    e_d, d_pd = sampling.sampler(S, nb, 1, field_source=ListSource(fields, uni)).propagate_phaseless(
+        ham, d_ham, d_prop, d_pd, d_trial, d_wave)
+    assert abs(float(e_d) - e_o) < 1e-4  # 0.1 mHa
