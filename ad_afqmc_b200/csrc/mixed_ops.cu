@@ -429,18 +429,25 @@ int mixed_fb_gemm(const Layout& L, const double* prep, double* work, cudaStream_
                       (long long)L.G * L.Kb, BN);
   if (rc != AFQ_OK) return rc;
   base_shape(P, L.npc, (int)M, L.G, (int)K, 1, BN, err_flag(L, work));
+  // every split owns at least one K block; partial buffers beyond the last
+  // split are zeroed so that the consumer's fixed-order sum stays exact
   const long long kblocks = (K + kUBK - 1) / kUBK;
   const long long per = (kblocks + L.splitk - 1) / L.splitk;
-  P.s.ksplit = L.splitk;
+  const int ks = (int)((kblocks + per - 1) / per);
+  P.s.ksplit = ks;
   P.s.kchunk = (int)(per * kUBK);
+  for (int z = ks; z < L.splitk; ++z)
+    if (cudaMemsetAsync(work + L.w_fbpart + z * 2LL * L.W * L.Gpad, 0,
+                        sizeof(double) * 2LL * L.W * L.Gpad, st) != cudaSuccess)
+      return AFQ_ERR_CUDA;
   P.epi.part = work + L.w_fbpart;
   P.epi.ld = L.Gpad;
   P.epi.zstride = 2LL * L.W * L.Gpad;
   return run<BN>(P, 0, st, K_FB);
 }
 
-int mixed_vhs_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {
-  constexpr int BN = 256;
+template <int BN>
+int vhs_launch(const Layout& L, const double* prep, double* work, cudaStream_t st) {
   UmmaParams<VhsEpiU> P{};
   bf16* a[3];
   bf16* b[3];
@@ -457,6 +464,11 @@ int mixed_vhs_gemm(const Layout& L, const double* prep, double* work, cudaStream
   P.epi.ld = L.Kv;
   P.epi.wstride = (long long)L.N * L.Kv;
   return run<BN>(P, 0, st, K_VHS);
+}
+
+int mixed_vhs_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {
+  // two pieces: 256-wide tiles (96 KB per stage); three pieces: 128-wide
+  return L.npc == 2 ? vhs_launch<256>(L, prep, work, st) : vhs_launch<128>(L, prep, work, st);
 }
 
 template <int BN>

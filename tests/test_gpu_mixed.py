@@ -44,7 +44,8 @@ CASES = [
     (48, (13, 11), 200, "uhf", "unrestricted", 24),
     (200, (40, 40), 1000, "rhf", "restricted", 8),
 ]
-TOL = {"mixed": 1e-4, "mixed_hi": 5e-6}
+# BF16x6 is limited by FP32 accumulation over K (up to 8000 in the force bias)
+TOL = {"mixed": 1e-4, "mixed_hi": 2e-5}
 
 
 @pytest.mark.parametrize("precision", ["mixed", "mixed_hi"])
