@@ -75,6 +75,7 @@ _SIGS = {
     "afq_small_workspace_size": ([C.POINTER(afq_dims), C.POINTER(C.c_size_t)], C.c_int),
     "afq_prepare": ([C.POINTER(afq_dims), C.POINTER(afq_ham), C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
     "afq_calc_overlap": ([C.POINTER(afq_dims), C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_calc_overlap_static": ([C.POINTER(afq_dims), C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_void_p], C.c_int),
     "afq_calc_green": ([C.POINTER(afq_dims), C.c_void_p * 2, C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
     "afq_calc_force_bias": ([C.POINTER(afq_dims), C.c_void_p, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
     "afq_calc_energy": ([C.POINTER(afq_dims), C.c_void_p, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),

@@ -132,6 +132,7 @@ const char* afq_status_string(int status) {
     case AFQ_ERR_WORKSPACE: return "prepared/workspace buffer too small";
     case AFQ_ERR_ALIGN: return "pointer not 16-byte aligned";
     case AFQ_ERR_ARG: return "argument out of range";
+    case AFQ_ERR_LIMIT: return "size exceeds the fixed static scratch capacity";
     default: return "unknown status";
   }
 }

@@ -41,7 +41,8 @@ typedef enum afq_status {
   AFQ_ERR_CUDA = 3,       /* CUDA runtime error during launch             */
   AFQ_ERR_WORKSPACE = 4,  /* prepared/workspace buffer too small          */
   AFQ_ERR_ALIGN = 5,      /* a pointer is not 16-byte aligned             */
-  AFQ_ERR_ARG = 6         /* an enum/flag argument is out of range        */
+  AFQ_ERR_ARG = 6,        /* an enum/flag argument is out of range        */
+  AFQ_ERR_LIMIT = 7       /* size beyond a fixed (static) scratch capacity */
 } afq_status;
 
 enum { AFQ_RESTRICTED = 0, AFQ_UNRESTRICTED = 1 };      /* walker_type  */
@@ -118,6 +119,20 @@ int afq_small_workspace_size(const afq_dims* d, size_t* bytes);
  * uhf._calc_overlap_unrestricted (:1259-1268). */
 int afq_calc_overlap(const afq_dims* d, const double* const mo[2], const double* const walkers[2],
                      double* overlaps, void* work, size_t work_bytes, void* stream);
+
+/* Overlaps like afq_calc_overlap, for callers that cannot allocate device
+ * memory: no workspace argument, and nothing is allocated.  No counterpart in
+ * the reference.  Host frameworks that own the device memory pool (an XLA
+ * custom call inside a JAX program, for one) or code recording into a CUDA
+ * graph under a capture mode that forbids allocation cannot pass a workspace;
+ * this entry point keeps its per-walker scratch in a fixed 1 MiB array inside
+ * the library's device image (held on every GPU that loads the library until
+ * the process exits).  Limit: nwalkers <= 8192, else AFQ_ERR_LIMIT.  The
+ * first call on a device looks up the array's device address; make it before
+ * any stream capture.  Calls share the array, so calls that overlap on the
+ * GPU race; nothing in it needs to start at zero. */
+int afq_calc_overlap_static(const afq_dims* d, const double* const mo[2],
+                            const double* const walkers[2], double* overlaps, void* stream);
 
 /* half-rotated Green's function per spin, (W, nocc[s], N) complex128 each.
  * Replaces rhf._calc_green (wavefunctions.py:1089-1100), uhf._calc_green (:1289-1312). */
