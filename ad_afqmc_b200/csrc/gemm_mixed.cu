@@ -70,13 +70,13 @@ struct StoreF32Epi {
   float* C;
   long long ldc, bstride;
   template <int BN>
-  __device__ void tile(int b, int mti, int nti, int row, uint32_t taddr, const UmmaShape& s,
+  __device__ void tile(int b, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t*) const {
     const int m = mti * s.a_step + row;
 #pragma unroll 1
     for (int ch = 0; ch < BN / 16; ++ch) {
       float v[16];
-      tmem_ld16(taddr + ch * 16, v);
+      src.load16(ch * 16, v);
       const int n0 = nti * s.b_step + ch * 16;
       if (m >= s.M) continue;
       float* r = C + b * bstride + (long long)m * ldc;
@@ -160,6 +160,8 @@ int afq_gemm_split_bf16(const void* const a_pieces[3], int npa, const void* cons
     if (rc != AFQ_OK) return rc;
   }
   P.s.a_batched = 1;
+  P.s.ngroups = 1;
+  P.s.kc = 0;
   P.s.stages = umma_pick_stages(BN, npa, npb, 0);
   P.s.M = M;
   P.s.N = N;

@@ -30,19 +30,24 @@ struct UExchTile {
   int bn, gpt, wpt, mt;
 };
 
-// Largest column tile that holds whole walkers and leaves room for two
+// Column tile of the exchange (two accumulator groups, double buffered:
+// BN <= 128) holding whole walkers with the least padding, with room for two
 // pipeline stages plus the epilogue's staging of one walker's f block.
 inline UExchTile choose_uexch_tile(int no, int G, int npc) {
   UExchTile t;
-  const int bns[4] = {240, 160, 128, 80};
+  const int bns[5] = {128, 96, 80, 64, 32};
   const long long budget = 227 * 1024 - 1024 - 256;
   const long long extra = ((128LL * (2 * no + 1) * 4 + 31) & ~31LL) + 128 * 32 + 128 * 16;
   t.bn = 0;
-  for (int i = 0; i < 4 && !t.bn; ++i) {
+  double best = -1.0;
+  for (int i = 0; i < 5; ++i) {
     const int bn = bns[i];
     if (((2 * no + 15) & ~15) > bn) continue;
     const long long stage = (long long)npc * (128 * 128 + bn * 128);
-    if (2 * stage + extra <= budget) t.bn = bn;
+    if (2 * stage + extra > budget) continue;
+    const int wpt = bn / (2 * no);
+    const double eff = double(wpt * 2 * no) / bn;
+    if (eff > best + 1e-9) { best = eff; t.bn = bn; }
   }
   t.gpt = 128 / no;
   t.wpt = t.bn ? t.bn / (2 * no) : 0;
@@ -202,7 +207,7 @@ inline int make_layout(const afq_dims* d, Layout& L) {
   L.w_xt = take(2 * W * L.Gpad);
   L.w_wscal = take(W * 16);
   L.w_vhs = take(W * N * 2 * L.Npad);
-  const long long pb = W * N * 2 * L.nomax;
+  const long long pb = W * N * 2 * L.nomax;  // (fp64 path) y / acc / t buffers
   L.w_y = take(pb);
   L.w_acc = take(pb);
   L.w_ta = take(pb);

@@ -51,14 +51,18 @@ inline int pairs_for(int npc, int* pa, int* pb) {
 // ---------------------------------------------------------------------------
 // operand preparation
 // ---------------------------------------------------------------------------
+// sub_identity: split (src - I) instead of src (square matrices)
 __global__ void split2d_kernel(const double* src, long long rows, long long cols, long long lds,
-                               int np, bf16* p0, bf16* p1, bf16* p2, long long ldd) {
+                               int np, bf16* p0, bf16* p1, bf16* p2, long long ldd,
+                               int sub_identity) {
   bf16* P[3] = {p0, p1, p2};
   const long long n = rows * cols;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
        e += (long long)gridDim.x * blockDim.x) {
     const long long r = e / cols, c = e - r * cols;
-    put_pieces(src[r * lds + c], np, P, r * ldd + c);
+    double x = src[r * lds + c];
+    if (sub_identity && r == c) x -= 1.0;
+    put_pieces(x, np, P, r * ldd + c);
   }
 }
 
@@ -81,7 +85,7 @@ __global__ void transpose_split_kernel(const double* src, long long R, long long
 
 // walker (W, N, nc) doubles -> pieces of its transpose (W, nc rows, K = N) with row stride ld
 __global__ void walker_t_kernel(const double* wk, int N, int nc, int np, bf16* p0, bf16* p1,
-                                bf16* p2, long long ld, long long bstride) {
+                                bf16* p2, long long ld, long long bstride, float* acc) {
   __shared__ double tile[32][33];
   bf16* P[3] = {p0, p1, p2};
   const int b = blockIdx.z;
@@ -94,30 +98,36 @@ __global__ void walker_t_kernel(const double* wk, int N, int nc, int np, bf16* p
   __syncthreads();
   for (int i = threadIdx.y; i < 32; i += blockDim.y) {
     const int n = n0 + i, p = p0_ + threadIdx.x;
-    if (n < nc && p < N) put_pieces(tile[threadIdx.x][i], np, P, (long long)b * bstride + (long long)n * ld + p);
+    if (n < nc && p < N) {
+      const double x = tile[threadIdx.x][i];
+      put_pieces(x, np, P, (long long)b * bstride + (long long)n * ld + p);
+      acc[((long long)b * nc + n) * N + p] = (float)x;  // identity term of the first half-step
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // epilogues
 // ---------------------------------------------------------------------------
+// C^T: rows g (Cholesky vector) = TMEM lanes, columns (w, re/im); the partial
+// sums land in part[z][(w,c)][g] so that a warp's stores are contiguous in g
 struct FbEpiU {
   double* part;
   long long ld, zstride;
   template <int BN>
-  __device__ void tile(int z, int mti, int nti, int row, uint32_t taddr, const UmmaShape& s,
+  __device__ void tile(int z, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t*) const {
-    const int m = mti * s.a_step + row;
-    double* dst = part + (long long)z * zstride + (long long)m * ld;
+    const int g = mti * s.a_step + row;
+    double* dst = part + (long long)z * zstride + g;
 #pragma unroll 1
     for (int ch = 0; ch < BN / 16; ++ch) {
       float v[16];
-      tmem_ld16(taddr + ch * 16, v);
-      if (m >= s.M) continue;
+      src.load16(ch * 16, v);
+      if (g >= s.M) continue;
       const int n0 = nti * s.b_step + ch * 16;
 #pragma unroll
       for (int i = 0; i < 16; ++i)
-        if (n0 + i < s.N) dst[n0 + i] = (double)v[i];
+        if (n0 + i < s.N) dst[(long long)(n0 + i) * ld] = (double)v[i];
     }
   }
 };
@@ -127,14 +137,14 @@ struct VhsEpiU {
   int npc, N;
   long long ld, wstride;
   template <int BN>
-  __device__ void tile(int, int mti, int nti, int row, uint32_t taddr, const UmmaShape& s,
+  __device__ void tile(int, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t*) const {
     const int q = mti * s.a_step + row;  // q = p*N + r
     const int p = q / N, r = q - (q / N) * N;
 #pragma unroll 1
     for (int ch = 0; ch < BN / 16; ++ch) {
       float v[16];
-      tmem_ld16(taddr + ch * 16, v);
+      src.load16(ch * 16, v);
       if (q >= s.M) continue;
       const int n0 = nti * s.b_step + ch * 16;
 #pragma unroll
@@ -149,55 +159,66 @@ struct VhsEpiU {
   }
 };
 
+// Modes of the propagator GEMMs.  The one-body factor is applied as
+// w + (e^{-dt h/2} - I) w: the tensor cores see only the small correction D
+// and the identity part is added exactly from the FP32 accumulator.
+//   PM_Y     v = D w      : acc = w + v = y ; next B <- [y^T | (i y)^T]
+//   PM_T     v = VHS t    : t = v/n ; acc += t ; next B <- [t^T | (i t)^T]
+//   PM_TLAST v = VHS t    : t = v/n ; acc += t ; next B <- acc^T (finished sum)
+//   PM_OUT   v = D acc    : walker = acc + v  (FP64 walker state)
 enum { PM_Y = 0, PM_T = 1, PM_TLAST = 2, PM_OUT = 3 };
 
 struct PropEpiU {
   int mode, npc, N, nc;
   float scale;
-  float* acc;           // (W, N, nc) fp32
+  float* acc;           // (W, nc, N) fp32, transposed so that a warp's lanes (rows p) are contiguous
   long long acc_bs;
   bf16* bt[3];          // next B operand: (W, nc rows, ld) pieces
   long long bt_ld, bt_bs;
   double* wout;         // (W, N, nc) doubles
   template <int BN>
-  __device__ void tile(int b, int mti, int, int row, uint32_t taddr, const UmmaShape& s,
+  __device__ void tile(int b, int mti, int, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t*) const {
     const int p = mti * s.a_step + row;
     const bool ok = p < N;
-    float* arow = acc + (long long)b * acc_bs + (long long)p * nc;
+    float* acol = acc + (long long)b * acc_bs + p;  // element (n, p) at acol[n * N]
     const long long bbase = (long long)b * bt_bs;
 #pragma unroll 1
     for (int ch = 0; ch < BN / 16; ++ch) {
       float v[16];
-      tmem_ld16(taddr + ch * 16, v);
+      src.load16(ch * 16, v);
       if (!ok) continue;
       const int n0 = ch * 16;
 #pragma unroll
       for (int i = 0; i < 16; i += 2) {
         const int n = n0 + i;  // (re, im) pair of orbital j = n/2
         if (n >= nc) break;
+        float* a0 = acol + (long long)n * N;
+        float* a1 = acol + (long long)(n + 1) * N;
         float tr = v[i], ti = v[i + 1];
         if (mode == PM_OUT) {
           double* o = wout + (long long)b * N * nc + (long long)p * nc + n;
-          o[0] = (double)tr;
-          o[1] = (double)ti;
+          o[0] = (double)(*a0 + tr);
+          o[1] = (double)(*a1 + ti);
           continue;
         }
-        if (mode != PM_Y) {
+        if (mode == PM_Y) {
+          tr += *a0;
+          ti += *a1;
+          *a0 = tr;
+          *a1 = ti;
+        } else {
           tr *= scale;
           ti *= scale;
+          const float sr = *a0 + tr, si = *a1 + ti;
+          *a0 = sr;
+          *a1 = si;
+          if (mode == PM_TLAST) {  // hand the finished sum to the closing half-step
+            tr = sr;
+            ti = si;
+          }
         }
-        if (mode == PM_Y) {
-          arow[n] = tr;
-          arow[n + 1] = ti;
-        } else if (mode == PM_T) {
-          arow[n] += tr;
-          arow[n + 1] += ti;
-        } else {  // last term: hand the finished sum to the closing half-step
-          tr += arow[n];
-          ti += arow[n + 1];
-        }
-        // t^T rows n (re) and n+1 (im); columns [0,N): t, [N,2N): i*t
+        // rows n (re) and n+1 (im) of the next B operand; columns [0,N): x, [N,2N): i*x
         put_pieces_f(tr, npc, bt, bbase + (long long)n * bt_ld + p);
         put_pieces_f(ti, npc, bt, bbase + (long long)(n + 1) * bt_ld + p);
         if (mode != PM_TLAST) {
@@ -214,7 +235,7 @@ struct ExchEpiU {
   double* cout;    // (W, G) complex
   double* excout;  // (mt, W) complex
   template <int BN>
-  __device__ void tile(int, int mti, int nti, int row, uint32_t taddr, const UmmaShape&,
+  __device__ void tile(int, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t* smem) const {
     const int nc = 2 * no, fs = nc + 1;
     float* Fs = reinterpret_cast<float*>(smem);
@@ -229,7 +250,7 @@ struct ExchEpiU {
       const int c_lo = cb & ~15, c_hi = (cb + nc + 15) & ~15;
       for (int c = c_lo; c < c_hi; c += 16) {
         float v[16];
-        tmem_ld16(taddr + c, v);
+        src.load16(c, v);
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
           const int col = c + k - cb;
@@ -316,12 +337,20 @@ void base_shape(UmmaParams<Epi>& P, int npc, int M, int N, int K, int batch, int
   P.s.nt = (N + bn - 1) / bn;
   P.s.ksplit = 1;
   P.s.kchunk = (K + kUBK - 1) / kUBK * kUBK;
+  P.s.ngroups = 1;
+  P.s.kc = 0;
   P.s.err = err;
 }
 
 template <int BN, class Epi>
 int run(UmmaParams<Epi>& P, size_t extra, cudaStream_t st, int prof_id) {
   P.s.stages = umma_pick_stages(BN, P.s.npa, P.s.npb, extra);
+  if (P.s.stages < 2 && P.s.kc > 0 && extra == umma_chunk_stage_bytes(BN)) {
+    // no room for the chunk staging next to two stages: accumulate in one chunk
+    P.s.kc = 0;
+    extra = 0;
+    P.s.stages = umma_pick_stages(BN, P.s.npa, P.s.npb, extra);
+  }
   if (P.s.stages < 2) return AFQ_ERR_SHAPE;
   ProfScope ps(prof_id, st);
   return launch_umma<BN>(P, extra, sm_count(), st) == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
@@ -355,7 +384,9 @@ int prop_launch(const Layout& L, const double* prep, double* work, int s, int nc
   P.epi.bt_ld = L.Kv;
   P.epi.bt_bs = btbs;
   P.epi.wout = wout;
-  return run<BN>(P, 0, st, K_PROP);
+  P.s.ngroups = 2;
+  P.s.kc = 4;
+  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_PROP);
 }
 
 template <int BN>
@@ -372,6 +403,7 @@ int exch_launch(const Layout& L, const double* prep, double* work, int s, cudaSt
                       L.Nb, brows * L.Nb, BN);
   if (rc != AFQ_OK) return rc;
   base_shape(P, L.npc, (int)arows, (int)brows, L.N, 1, BN, err_flag(L, work));
+  P.s.ngroups = 2;  // hi x hi products apart from the cross terms: shorter rounding chains
   P.s.a_step = X.gpt * no;
   P.s.b_step = X.wpt * 2 * no;
   P.s.mt = X.mt;
@@ -394,7 +426,7 @@ int mixed_prepare(const Layout& L, double* P, cudaStream_t st) {
   // force-bias operand: rot_chol concatenated over spins (G x Kfb)
   piece_ptrs(P, L.q_rccat, L.q_rccat_ps, L.npc, q);
   split2d_kernel<<<1184, 256, 0, st>>>(P + L.p_rccat, L.G, L.Kfb_used, L.Kfb, L.npc, q[0], q[1],
-                                       q[2], L.Kb);
+                                       q[2], L.Kb, 0);
   // VHS operand: chol transposed to (N^2 x G)
   piece_ptrs(P, L.q_cholT, L.q_cholT_ps, L.npc, q);
   {
@@ -405,14 +437,15 @@ int mixed_prepare(const Layout& L, double* P, cudaStream_t st) {
   }
   for (int s = 0; s < L.np; ++s) {
     piece_ptrs(P, L.q_exph1[s], L.q_exph1_ps, L.npc, q);
+    // the propagator applies e^{-dt h/2} as w + (e^{-dt h/2} - I) w
     split2d_kernel<<<296, 256, 0, st>>>(P + L.p_exph1[s], L.N, L.N, L.Npad, L.npc, q[0], q[1],
-                                        q[2], L.Nb);
+                                        q[2], L.Nb, 1);
   }
   const int ntr = L.uhf_trial ? 2 : 1;
   for (int s = 0; s < ntr; ++s) {
     piece_ptrs(P, L.q_rc[s], L.q_rc_ps[s], L.npc, q);
     split2d_kernel<<<1184, 256, 0, st>>>(P + L.p_rc[s], (long long)L.G * L.no[s], L.N, L.Npad,
-                                         L.npc, q[0], q[1], q[2], L.Nb);
+                                         L.npc, q[0], q[1], q[2], L.Nb, 0);
   }
   return cudaGetLastError() == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
 }
@@ -422,13 +455,13 @@ int mixed_fb_gemm(const Layout& L, const double* prep, double* work, cudaStream_
   UmmaParams<FbEpiU> P{};
   bf16* a[3];
   bf16* b[3];
-  piece_ptrs(work, L.v_gpl, L.v_gpl_ps, L.npc, a);
-  piece_ptrs(const_cast<double*>(prep), L.q_rccat, L.q_rccat_ps, L.npc, b);
-  const long long K = L.Kfb_used, M = 2LL * L.W;
-  int rc = setup_maps(P, a, L.npc, K, M, 1, L.Kb, M * L.Kb, b, L.npc, K, L.G, 1, L.Kb,
-                      (long long)L.G * L.Kb, BN);
+  piece_ptrs(const_cast<double*>(prep), L.q_rccat, L.q_rccat_ps, L.npc, a);
+  piece_ptrs(work, L.v_gpl, L.v_gpl_ps, L.npc, b);
+  const long long K = L.Kfb_used, N2 = 2LL * L.W;
+  int rc = setup_maps(P, a, L.npc, K, L.G, 1, L.Kb, (long long)L.G * L.Kb, b, L.npc, K, N2, 1,
+                      L.Kb, N2 * L.Kb, BN);
   if (rc != AFQ_OK) return rc;
-  base_shape(P, L.npc, (int)M, L.G, (int)K, 1, BN, err_flag(L, work));
+  base_shape(P, L.npc, L.G, (int)N2, (int)K, 1, BN, err_flag(L, work));
   // every split owns at least one K block; partial buffers beyond the last
   // split are zeroed so that the consumer's fixed-order sum stays exact
   const long long kblocks = (K + kUBK - 1) / kUBK;
@@ -443,7 +476,9 @@ int mixed_fb_gemm(const Layout& L, const double* prep, double* work, cudaStream_
   P.epi.part = work + L.w_fbpart;
   P.epi.ld = L.Gpad;
   P.epi.zstride = 2LL * L.W * L.Gpad;
-  return run<BN>(P, 0, st, K_FB);
+  P.s.ngroups = 2;
+  P.s.kc = 4;
+  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_FB);
 }
 
 template <int BN>
@@ -463,12 +498,15 @@ int vhs_launch(const Layout& L, const double* prep, double* work, cudaStream_t s
   P.epi.N = L.N;
   P.epi.ld = L.Kv;
   P.epi.wstride = (long long)L.N * L.Kv;
-  return run<BN>(P, 0, st, K_VHS);
+  // K = G accumulates in chunks of 4 K blocks, the hi x hi product apart
+  P.s.ngroups = 2;
+  P.s.kc = 4;
+  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_VHS);
 }
 
 int mixed_vhs_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {
-  // two pieces: 256-wide tiles (96 KB per stage); three pieces: 128-wide
-  return L.npc == 2 ? vhs_launch<256>(L, prep, work, st) : vhs_launch<128>(L, prep, work, st);
+  // two pieces: 128-wide tiles; three pieces: 64-wide (both keep chunked accumulation)
+  return L.npc == 2 ? vhs_launch<128>(L, prep, work, st) : vhs_launch<64>(L, prep, work, st);
 }
 
 template <int BN>
@@ -485,7 +523,7 @@ static int propagate_one(const Layout& L, const double* prep, double* work, doub
     ProfScope ps(K_MISC, st);
     dim3 grid((N + 31) / 32, (nc + 31) / 32, L.W);
     walker_t_kernel<<<grid, dim3(32, 8), 0, st>>>(wk, N, nc, L.npc, b0[0], b0[1], b0[2], L.Kv,
-                                                  btbs);
+                                                  btbs, reinterpret_cast<float*>(work + L.v_acc));
     if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
   }
   const long long vbs = (long long)N * L.Kv;
@@ -542,10 +580,11 @@ int mixed_propagate_walkers(const Layout& L, const double* prep, double* work,
 
 int mixed_exchange(const Layout& L, const double* prep, double* work, int s, cudaStream_t st) {
   switch (L.uex[s].bn) {
-    case 240: return exch_launch<240>(L, prep, work, s, st);
-    case 160: return exch_launch<160>(L, prep, work, s, st);
     case 128: return exch_launch<128>(L, prep, work, s, st);
-    default: return exch_launch<80>(L, prep, work, s, st);
+    case 96: return exch_launch<96>(L, prep, work, s, st);
+    case 80: return exch_launch<80>(L, prep, work, s, st);
+    case 64: return exch_launch<64>(L, prep, work, s, st);
+    default: return exch_launch<32>(L, prep, work, s, st);
   }
 }
 

@@ -152,6 +152,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 16 columns of the accumulator, summing the second accumulator group (if
+// any, BN columns further on) in FP32 round-to-nearest
+__device__ __forceinline__ void acc_ld16(uint32_t taddr, int ngroups, int bn, float (&v)[16]) {
+  tmem_ld16(taddr, v);
+  if (ngroups == 2) {
+    float w[16];
+    tmem_ld16(taddr + bn, w);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] += w[i];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // tcgen05.mma (single CTA, A and B from shared memory)
 // ---------------------------------------------------------------------------

@@ -34,8 +34,32 @@ struct UmmaShape {
   int npa, npb;      // pieces of A and B
   int npairs;
   int pa[6], pb[6];
+  int ngroups;       // 1, or 2: pair 0 (the hi x hi product) accumulates apart from the rest
+  int kc;            // K blocks per accumulator chunk (0: the whole K of a tile in one chunk)
   int* err;          // device error flag (set to 1 on a timed-out wait)
 };
+
+// Where an epilogue reads the finished accumulator of its row: straight from
+// TMEM (one chunk; two groups summed) or from the FP32 shared-memory row that
+// summed the chunks with round-to-nearest adds.
+struct AccSrc {
+  uint32_t taddr;
+  int ngroups, bn;
+  const float* srow;  // nullptr: read TMEM
+  __device__ __forceinline__ void load16(int col, float (&v)[16]) const {
+    if (srow) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[i] = srow[col + i];
+    } else {
+      acc_ld16(taddr + col, ngroups, bn, v);
+    }
+  }
+};
+
+// FP32 staging for chunked accumulation: one (BN+1)-float row per TMEM lane
+__host__ __device__ inline size_t umma_chunk_stage_bytes(int bn) {
+  return size_t(128) * (bn + 1) * sizeof(float);
+}
 
 template <class Epi>
 struct UmmaParams {
@@ -45,9 +69,10 @@ struct UmmaParams {
   Epi epi;
 };
 
-__host__ __device__ constexpr int umma_tmem_cols(int bn) {
+// TMEM columns for two accumulator buffers of ngroups x bn fp32 columns
+__host__ __device__ constexpr int umma_tmem_cols(int bn, int ngroups = 1) {
   int c = 32;
-  while (c < 2 * bn) c <<= 1;
+  while (c < 2 * ngroups * bn) c <<= 1;
   return c;
 }
 
@@ -85,7 +110,8 @@ __global__ void __launch_bounds__(192, 1) umma_gemm_kernel(const __grid_constant
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce + 2);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
   uint8_t* epi_smem = reinterpret_cast<uint8_t*>(full) + 256;  // epilogue scratch
-  constexpr uint32_t kCols = umma_tmem_cols(BN);
+  const uint32_t kCols = umma_tmem_cols(BN, P.s.ngroups);
+  const uint32_t acc_stride = (uint32_t)(P.s.ngroups * BN);  // columns per accumulator buffer
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -151,51 +177,85 @@ __global__ void __launch_bounds__(192, 1) umma_gemm_kernel(const __grid_constant
       int stage = 0;
       uint32_t phase = 0;
       int it = 0;
-      for (int tile = blockIdx.x; tile < tiles && !*abort_s; tile += gridDim.x, ++it) {
-        const int buf = it & 1;
-        const uint32_t use = (uint32_t)(it >> 1);
-        if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); break; }
-        tc_fence_after();
-        const uint32_t dt = tbase + buf * BN;
+      for (int tile = blockIdx.x; tile < tiles && !*abort_s; tile += gridDim.x) {
         const int k0 = ((tile / (S.nt * S.mt)) % S.ksplit) * S.kchunk;
         const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
+        const int kc = S.kc > 0 ? S.kc : KB;
         bool ok = true;
-        for (int kb = 0; kb < KB; ++kb) {
-          if (!mbar_wait(&full[stage], phase)) { fail(); ok = false; break; }
+        for (int c0 = 0; c0 < KB && ok; c0 += kc, ++it) {
+          const int buf = it & 1;
+          const uint32_t use = (uint32_t)(it >> 1);
+          if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); ok = false; break; }
           tc_fence_after();
-          const uint8_t* sa = smem + stage * stage_bytes;
-          const uint8_t* sb = sa + S.npa * a_bytes;
-          for (int p = 0; p < S.npairs; ++p) {
-            const uint64_t ad = smem_desc_sw128(sa + S.pa[p] * a_bytes);
-            const uint64_t bd = smem_desc_sw128(sb + S.pb[p] * b_bytes);
+          const uint32_t dt = tbase + buf * acc_stride;
+          const int c1 = min(KB, c0 + kc);
+          for (int kb = c0; kb < c1; ++kb) {
+            if (!mbar_wait(&full[stage], phase)) { fail(); ok = false; break; }
+            tc_fence_after();
+            const uint8_t* sa = smem + stage * stage_bytes;
+            const uint8_t* sb = sa + S.npa * a_bytes;
+            for (int p = 0; p < S.npairs; ++p) {
+              const uint64_t ad = smem_desc_sw128(sa + S.pa[p] * a_bytes);
+              const uint64_t bd = smem_desc_sw128(sb + S.pb[p] * b_bytes);
+              // group 0: pair 0 alone; group 1 (if any): the remaining pairs
+              const int grp = (S.ngroups == 2 && p > 0) ? 1 : 0;
+              const int first = (p == 0) || (S.ngroups == 2 && p == 1);
 #pragma unroll
-            for (int ks = 0; ks < kUBK / 16; ++ks)
-              umma_bf16(dt, ad + 2 * ks, bd + 2 * ks, idesc, (kb | p | ks) != 0);
+              for (int ks = 0; ks < kUBK / 16; ++ks)
+                umma_bf16(dt + grp * BN, ad + 2 * ks, bd + 2 * ks, idesc,
+                          (kb - c0) != 0 || ks != 0 || !first);
+            }
+            umma_commit(&empty[stage]);
+            if (++stage == ST) { stage = 0; phase ^= 1; }
           }
-          umma_commit(&empty[stage]);
-          if (++stage == ST) { stage = 0; phase ^= 1; }
+          if (!ok) break;
+          umma_commit(&accf[buf]);
         }
         if (!ok) break;
-        umma_commit(&accf[buf]);
       }
     }
   } else {
     const int sub = warp & 3;
     const int row = sub * 32 + lane;
+    float* srow = reinterpret_cast<float*>(epi_smem) + row * (BN + 1);
     int it = 0;
-    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
-      const int buf = it & 1;
-      const uint32_t use = (uint32_t)(it >> 1);
-      if (!mbar_wait_abortable(&accf[buf], use & 1, abort_s)) { fail(); break; }
-      tc_fence_after();
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
       const int nti = tile % S.nt, rest = tile / S.nt;
       const int mti = rest % S.mt, z = rest / S.mt;
-      // z = batch * ksplit + split
-      P.epi.template tile<BN>(z, mti, nti, row, tbase + ((uint32_t)(sub * 32) << 16) + buf * BN, S,
-                              epi_smem);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acce[buf]);
+      const int k0 = (z % S.ksplit) * S.kchunk;
+      const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
+      const int kc = S.kc > 0 ? S.kc : KB;
+      const int nch = (KB + kc - 1) / kc;
+      for (int ch = 0; ch < nch; ++ch, ++it) {
+        const int buf = it & 1;
+        const uint32_t use = (uint32_t)(it >> 1);
+        if (!mbar_wait_abortable(&accf[buf], use & 1, abort_s)) { fail(); ok = false; break; }
+        tc_fence_after();
+        const uint32_t taddr = tbase + ((uint32_t)(sub * 32) << 16) + buf * acc_stride;
+        if (nch == 1) {
+          // z = batch * ksplit + split
+          P.epi.template tile<BN>(z, mti, nti, row, AccSrc{taddr, S.ngroups, BN, nullptr}, S,
+                                  epi_smem);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acce[buf]);
+        } else {
+#pragma unroll 1
+          for (int c = 0; c < BN / 16; ++c) {
+            float v[16];
+            acc_ld16(taddr + c * 16, S.ngroups, BN, v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              srow[c * 16 + i] = (ch == 0) ? v[i] : srow[c * 16 + i] + v[i];
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acce[buf]);
+          if (ch == nch - 1)
+            P.epi.template tile<BN>(z, mti, nti, row, AccSrc{0u, 1, BN, srow}, S, epi_smem);
+        }
+      }
     }
   }
   tc_fence_before();

@@ -44,7 +44,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed_hi"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_hi"])
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the FP64 comparison leg and the block-energy error check")
     ap.add_argument("--config", default=CONFIG)
     ap.add_argument("--walkers", type=int, default=0, help="override walker count")
     ap.add_argument("--no-e2e", action="store_true")
@@ -189,54 +191,93 @@ def main():
 
     trial = wavefunctions.rhf(sys_.norb, sys_.nelec) if sys_.trial == "rhf" else wavefunctions.uhf(sys_.norb, sys_.nelec)
     wt = "restricted" if sys_.trial == "rhf" else "unrestricted"
-    ham_data, wave = sys_.ham_data(), sys_.wave_data()
     ham = hamiltonian.hamiltonian(sys_.norb)
-    prop = propagation.propagator_afqmc(dt=dt, n_walkers=W, walker_type=wt, precision=args.precision)
-    ham_data = ham.build_measurement_intermediates(ham_data, trial, wave)
-    ham_data = ham.build_propagation_intermediates(ham_data, prop, trial, wave)
-    pd = prop.init_prop_data(trial, wave, ham_data, seed=1000 + rank)
-    smp = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1)
 
-    def one_block(pd, e_acc=None):
-        e, pd = smp.propagate_phaseless(ham, ham_data, prop, pd, trial, wave)
+    def setup(system, precision, seed):
+        hd, wv = system.ham_data(), system.wave_data()
+        pr = propagation.propagator_afqmc(dt=dt, n_walkers=W, walker_type=wt, precision=precision)
+        hd = ham.build_measurement_intermediates(hd, trial, wv)
+        hd = ham.build_propagation_intermediates(hd, pr, trial, wv)
+        pd_ = pr.init_prop_data(trial, wv, hd, seed=seed)
+        return hd, wv, pr, pd_
+
+    def one_block(smp_, hd, wv, pr, pd_):
+        e, pd_ = smp_.propagate_phaseless(ham, hd, pr, pd_, trial, wv)
         if world > 1:
-            t = torch.stack([e * torch.sum(pd["weights"]), torch.sum(pd["weights"])])
+            t = torch.stack([e * torch.sum(pd_["weights"]), torch.sum(pd_["weights"])])
             dist.all_reduce(t)
-        pd["e_estimate"] = 0.9 * pd["e_estimate"] + 0.1 * e
-        return pd, e
+        pd_["e_estimate"] = 0.9 * pd_["e_estimate"] + 0.1 * e
+        return pd_, e
 
-    for _ in range(args.warmup):
-        pd, _ = one_block(pd)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    def timed_run(precision, steps, warmup, profile_kernel=None):
+        hd, wv, pr, pd_ = setup(sys_, precision, 1000 + rank)
+        smp_ = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1)
+        for _ in range(warmup):
+            pd_, _ = one_block(smp_, hd, wv, pr, pd_)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        n0 = _lib.launch_count()
+        if profile_kernel:
+            _lib.profile_begin(profile_kernel)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(steps):
+            pd_, _ = one_block(smp_, hd, wv, pr, pd_)
+        stop.record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = start.elapsed_time(stop)
+        kern = _lib.profile_end() if profile_kernel else (0.0, 0)
+        launches = _lib.launch_count() - n0
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, kern, launches, float(pd_["n_killed_walkers"]), (hd, wv, pr, pd_)
 
     clk_path = os.path.join(tempfile.gettempdir(), f"afq_clocks_{rank}.csv")
     clk = clocks_start(clk_path)
-    n0 = _lib.launch_count()
-    dominant = "vhs"
-    _lib.profile_begin(dominant)
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    start.record()
-    energies = []
-    for _ in range(args.steps):
-        pd, e = one_block(pd)
-        energies.append(e)
-    stop.record()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ms_total = start.elapsed_time(stop)
-    kern_ms, kern_n = _lib.profile_end()
-    launches = _lib.launch_count() - n0
+    ms_total, (kern_ms, kern_n), launches, killed, (ham_data, wave, prop, pd) = timed_run(
+        args.precision, args.steps, args.warmup, "vhs")
     clocks = clocks_stop(clk, clk_path, torch.cuda.current_device())
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
     value = world * W * S * args.steps / (ms_total / 1e3)
-    killed = float(pd["n_killed_walkers"])
+
+    # ---- FP64 GPU path on the same workload, and the block-energy error -------
+    compare = None
+    if not args.no_compare and args.precision != "fp64":
+        ms64, _, _, _, _ = timed_run("fp64", max(2, args.steps // 2), 1)
+        v64 = world * W * S * max(2, args.steps // 2) / (ms64 / 1e3)
+        # same-shape system with a surviving population (Cholesky vectors x0.25):
+        # identical walkers and device-drawn fields for both precisions
+        from ad_afqmc_b200.synthetic import make_config as _mk
+        sys_h, _ = _mk(args.config, chol_scale=0.25)
+        nb = 3
+        energies = {}
+        for precision in (args.precision, "fp64"):
+            hd, wv = sys_h.ham_data(), sys_h.wave_data()
+            pr = propagation.propagator_afqmc(dt=dt, n_walkers=W, walker_type=wt, precision=precision)
+            hd = ham.build_measurement_intermediates(hd, trial, wv)
+            hd = ham.build_propagation_intermediates(hd, pr, trial, wv)
+            pd_ = pr.init_prop_data(trial, wv, hd, seed=4242)
+            smp_ = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1)
+            es = []
+            for _ in range(nb):
+                pd_, e = one_block(smp_, hd, wv, pr, pd_)
+                es.append(float(e))
+            energies[precision] = (es, float(pd_["n_killed_walkers"]))
+            del hd, pr, pd_
+        err = max(abs(a - b) for a, b in zip(energies[args.precision][0], energies["fp64"][0]))
+        compare = {"fp64_value": v64, "fp64_ms_per_step": ms64 / max(2, args.steps // 2),
+                   "speedup_vs_fp64": value / v64,
+                   "block_energy_error_ha": err,
+                   "block_energy_check": f"{nb} blocks x {S} steps, {W} walkers, chol_scale 0.25, "
+                                         "same walkers and fields, vs the FP64 GPU path (which "
+                                         "matches the NumPy oracle to 1e-8 Ha)",
+                   "block_energies_fp64": energies["fp64"][0],
+                   "killed_fraction_check": energies[args.precision][1]}
 
     # ---- end to end through the public API with host buffers -------------
     e2e = None
@@ -321,7 +362,7 @@ def main():
                       "l2": "working set (VHS 328 MB, chol 320 MB) exceeds the 126 MB L2",
                       "chol_scale": args.chol_scale, "killed_walker_fraction": killed},
            "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-           "clocks": clocks}
+           "clocks": clocks, "compare": compare}
     print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()
