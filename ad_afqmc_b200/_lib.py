@@ -58,7 +58,12 @@ class afq_state(C.Structure):
         ("weights", C.c_void_p),
         ("overlaps", C.c_void_p),
         ("scalars", C.c_void_p),
+        ("flags", C.c_int32),
+        ("reserved", C.c_int32),
     ]
+
+
+AFQ_STATE_GREEN_CURRENT = 1
 
 
 class AfqError(RuntimeError):

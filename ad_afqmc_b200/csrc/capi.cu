@@ -282,10 +282,20 @@ int afq_propagate_constrained(const afq_dims* d, const void* prepared, afq_state
   const double* P = static_cast<const double*>(prepared);
   double* Wk = static_cast<double*>(work);
   cudaStream_t st = as_stream(stream);
-  // force bias of the current walkers
+  // force bias of the current walkers (the Green's function is reused when the
+  // previous step on this workspace already computed it for these walkers)
   GreenArgs a = green_args(L, P, Wk, wc);
-  rc = force_bias_impl(L, P, Wk, a, st);
-  if (rc != AFQ_OK) return rc;
+  if (s->flags & AFQ_STATE_GREEN_CURRENT) {
+    if (L.mixed) {
+      if ((rc = mixed_fb_gemm(L, P, Wk, st)) != AFQ_OK) return rc;
+    } else {
+      AFQ_TRY(launch_fb_gemm(L, P, Wk, st));
+    }
+  } else {
+    rc = force_bias_impl(L, P, Wk, a, st);
+    if (rc != AFQ_OK) return rc;
+  }
+  s->flags &= ~AFQ_STATE_GREEN_CURRENT;
   AFQ_TRY(launch_prep(L, P, Wk, fields, d->dt, nullptr, st));
   // VHS and the Trotterized propagator
   if (L.mixed) {
@@ -296,9 +306,14 @@ int afq_propagate_constrained(const afq_dims* d, const void* prepared, afq_state
     AFQ_TRY(launch_vhs_gemm(L, P, Wk, st));
     AFQ_TRY(launch_propagate_walkers(L, P, Wk, s->walkers, d->n_exp_terms, st));
   }
-  // new overlaps and the phaseless weight update
+  // new overlaps (and the next step's force-bias operand) and the weight update
   GreenArgs b = green_args(L, P, Wk, wc);
+  if (L.mixed)
+    piece_ptrs(Wk, L.v_gpl, L.v_gpl_ps, L.npc, b.gplb);
+  else
+    b.gpl = Wk + L.w_gpl;
   AFQ_TRY(launch_green(b, st));
+  s->flags |= AFQ_STATE_GREEN_CURRENT;
   AFQ_TRY(launch_ovlp_combine(L.W, L.ns, L.mult, Wk + L.w_wscal, Wk + L.w_wscal + 12, 16, st));
   AFQ_TRY(launch_weight_update(L, P, Wk, s->weights, s->overlaps, s->scalars, d->dt, st));
   return AFQ_OK;

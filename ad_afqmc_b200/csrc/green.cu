@@ -31,8 +31,10 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
 
   double2* S = sm;                          // no*no
   double2* colk = S + no * no;              // 64
-  double2* stage = colk + 64;               // kRowChunk*no
+  double2* stage = colk + 64;               // kRowChunk*no   (walker rows, C^T W phase)
   double* moc = reinterpret_cast<double*>(stage + kRowChunk * no);  // kRowChunk*no
+  double2* tstage = reinterpret_cast<double2*>(moc + kRowChunk * no);  // kRowChunk*(no+1)
+  const int ts = no + 1;  // padded row stride of tstage (conflict-free column reads)
   __shared__ double red[2 * (T / 32)];
   __shared__ int perm[64];
   __shared__ int piv_s;
@@ -157,9 +159,12 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
   const bool tb = S_.gtb[0] != nullptr;
   for (int p0 = 0; p0 < N; p0 += kRowChunk) {
     const int rows = min(kRowChunk, N - p0);
+    // walker rows of this chunk into shared memory
+    for (int e = tid; e < rows * no; e += T) stage[e] = Wg[(long long)p0 * no + e];
+    __syncthreads();
     for (int e = tid; e < rows * no; e += T) {
       const int r = e / no, j = e - (e / no) * no;
-      const double2* wrow = Wg + (long long)(p0 + r) * no;
+      const double2* wrow = stage + r * no;
       double2 s = make_double2(0.0, 0.0);
       for (int i = 0; i < no; ++i) {
         const double2 x = wrow[i];
@@ -167,7 +172,7 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
         s.x = fma(x.x, y.x, fma(-x.y, y.y, s.x));
         s.y = fma(x.x, y.y, fma(x.y, y.x, s.y));
       }
-      stage[e] = s;
+      tstage[r * ts + j] = s;
       if (th) th[(long long)(p0 + r) * no + j] = s;
       if (S_.rh1) {
         const double h = S_.rh1[(long long)j * N + p0 + r];
@@ -179,7 +184,7 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
     if (go || gre || gb || tb) {
       for (int e = tid; e < rows * no; e += T) {
         const int j = e / rows, r = e - (e / rows) * rows;
-        const double2 v = stage[r * no + j];
+        const double2 v = tstage[r * ts + j];
         if (go) go[(long long)j * N + p0 + r] = v;
         if (gre) {
           gre[(long long)j * N + p0 + r] = v.x;
@@ -231,7 +236,8 @@ cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   int nomax = 0;
   for (int s = 0; s < a.ns; ++s) nomax = a.sec[s].no > nomax ? a.sec[s].no : nomax;
   const size_t smem = (size_t(nomax) * nomax + 64 + kRowChunk * nomax) * sizeof(double2) +
-                      size_t(kRowChunk) * nomax * sizeof(double);
+                      size_t(kRowChunk) * nomax * sizeof(double) +
+                      size_t(kRowChunk) * (nomax + 1) * sizeof(double2);
   cudaError_t e = cudaFuncSetAttribute(green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;

@@ -37,7 +37,7 @@ inline UExchTile choose_uexch_tile(int no, int G, int npc) {
   UExchTile t;
   const int bns[5] = {128, 96, 80, 64, 32};
   const long long budget = 227 * 1024 - 1024 - 256;
-  const long long extra = ((128LL * (2 * no + 1) * 4 + 31) & ~31LL) + 128 * 32 + 128 * 16;
+  const long long extra = ((128LL * (2 * no + 2) * 4 + 31) & ~31LL) + 128 * 32 + 128 * 16;
   t.bn = 0;
   double best = -1.0;
   for (int i = 0; i < 5; ++i) {

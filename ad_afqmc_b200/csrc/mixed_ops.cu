@@ -189,6 +189,10 @@ struct PropEpiU {
       src.load16(ch * 16, v);
       if (!ok) continue;
       const int n0 = ch * 16;
+      // all accumulator loads of the chunk first (independent, in flight together)
+      float av[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) av[i] = (n0 + i < nc) ? acol[(long long)(n0 + i) * N] : 0.f;
 #pragma unroll
       for (int i = 0; i < 16; i += 2) {
         const int n = n0 + i;  // (re, im) pair of orbital j = n/2
@@ -198,19 +202,19 @@ struct PropEpiU {
         float tr = v[i], ti = v[i + 1];
         if (mode == PM_OUT) {
           double* o = wout + (long long)b * N * nc + (long long)p * nc + n;
-          o[0] = (double)(*a0 + tr);
-          o[1] = (double)(*a1 + ti);
+          o[0] = (double)(av[i] + tr);
+          o[1] = (double)(av[i + 1] + ti);
           continue;
         }
         if (mode == PM_Y) {
-          tr += *a0;
-          ti += *a1;
+          tr += av[i];
+          ti += av[i + 1];
           *a0 = tr;
           *a1 = ti;
         } else {
           tr *= scale;
           ti *= scale;
-          const float sr = *a0 + tr, si = *a1 + ti;
+          const float sr = av[i] + tr, si = av[i + 1] + ti;
           *a0 = sr;
           *a1 = si;
           if (mode == PM_TLAST) {  // hand the finished sum to the closing half-step
@@ -237,7 +241,7 @@ struct ExchEpiU {
   template <int BN>
   __device__ void tile(int, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t* smem) const {
-    const int nc = 2 * no, fs = nc + 1;
+    const int nc = 2 * no, fs = nc + 2;  // even stride: float2 reads of (re, im) pairs
     float* Fs = reinterpret_cast<float*>(smem);
     double4* pr = reinterpret_cast<double4*>(smem + ((128 * fs * 4 + 31) & ~31));
     double2* ge = reinterpret_cast<double2*>(pr + 128);
@@ -259,16 +263,19 @@ struct ExchEpiU {
       }
       named_sync_epi();
       if (valid) {
+        // sum_j f[i][j] f[j][i]: products in FP32, sums in FP64
         double er = 0.0, ei = 0.0;
-        const float* fr = Fs + row * fs;
+        const float2* fr = reinterpret_cast<const float2*>(Fs + row * fs);
         const float* fc = Fs + (gl * no) * fs + 2 * i;
+#pragma unroll 4
         for (int j = 0; j < no; ++j) {
-          const double ar = fr[2 * j], ai = fr[2 * j + 1];
-          const double br = fc[j * fs], bi = fc[j * fs + 1];
-          er += ar * br - ai * bi;
-          ei += ar * bi + ai * br;
+          const float2 a = fr[j];
+          const float2 b = *reinterpret_cast<const float2*>(fc + j * fs);
+          er += (double)(a.x * b.x) - (double)(a.y * b.y);
+          ei += (double)(a.x * b.y) + (double)(a.y * b.x);
         }
-        pr[row] = make_double4(er, ei, (double)fr[2 * i], (double)fr[2 * i + 1]);
+        const float2 d = fr[i];
+        pr[row] = make_double4(er, ei, (double)d.x, (double)d.y);
       }
       named_sync_epi();
       if (row < gcount) {
@@ -298,7 +305,7 @@ struct ExchEpiU {
     }
   }
   static size_t smem_extra(int no) {
-    const int fs = 2 * no + 1;
+    const int fs = 2 * no + 2;
     return ((size_t(128) * fs * 4 + 31) & ~size_t(31)) + 128 * sizeof(double4) + 128 * sizeof(double2);
   }
 };

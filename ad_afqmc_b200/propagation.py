@@ -83,7 +83,16 @@ def sync_scalars(prop_data: dict) -> torch.Tensor:
     return sc
 
 
-def make_state(prop_data: dict) -> _lib.afq_state:
+def _walker_key(prop_data: dict, eng) -> tuple:
+    w = prop_data["walkers"]
+    ptrs = tuple(t.data_ptr() for t in (w.data if isinstance(w, UHFWalkers) else [w.data]))
+    return (id(eng), id(w)) + ptrs
+
+
+def make_state(prop_data: dict, eng=None) -> _lib.afq_state:
+    """C-ABI state of prop_data.  The GREEN_CURRENT flag is set only when the
+    engine's workspace holds the Green's function of exactly these walker
+    tensors (left by the previous step); any new walker object clears it."""
     st = _lib.afq_state()
     w = prop_data["walkers"]
     if isinstance(w, UHFWalkers):
@@ -95,7 +104,18 @@ def make_state(prop_data: dict) -> _lib.afq_state:
     st.weights = prop_data["weights"].data_ptr()
     st.overlaps = prop_data["overlaps"].data_ptr()
     st.scalars = prop_data["_scalars"].data_ptr()
+    st.flags = 0
+    if eng is not None and prop_data.get("_afq_green_of") == _walker_key(prop_data, eng):
+        st.flags = _lib.AFQ_STATE_GREEN_CURRENT
     return st
+
+
+def note_state(prop_data: dict, st: _lib.afq_state, eng) -> None:
+    """Record, after a C call, whether the workspace holds these walkers' G."""
+    if st.flags & _lib.AFQ_STATE_GREEN_CURRENT:
+        prop_data["_afq_green_of"] = _walker_key(prop_data, eng)
+    else:
+        prop_data.pop("_afq_green_of", None)
 
 
 @dataclass
@@ -160,13 +180,14 @@ class propagator_afqmc(propagator):
         f = to_dev(fields, torch.float64)
         if f.shape != (self.n_walkers, int(ham_data["chol"].shape[0])):
             raise ValueError(f"fields must be (n_walkers, nchol), got {tuple(f.shape)}")
-        st = make_state(prop_data)
+        st = make_state(prop_data, eng)
         p, w, wb = eng.handle
         _lib.check(
             _lib.lib().afq_propagate_constrained(C.byref(eng.dims), p, C.byref(st), f.data_ptr(), w, wb,
                                                  _lib.stream_handle()),
             "afq_propagate_constrained",
         )
+        note_state(prop_data, st, eng)
         return prop_data
 
     def _build_propagation_intermediates(self, ham_data: dict, trial, wave_data: dict) -> dict:

@@ -23,7 +23,7 @@ import torch
 
 from . import _lib
 from ._engine import device, to_dev
-from .propagation import make_state, normal_fields, sync_scalars
+from .propagation import make_state, normal_fields, note_state, sync_scalars
 
 
 @dataclass
@@ -53,13 +53,15 @@ class sampler:
         p, w, wb = eng.handle
         lib = _lib.lib()
         stream = _lib.stream_handle()
-        st = make_state(prop_data)
+        st = make_state(prop_data, eng)
         for s in range(self.n_prop_steps):
             _lib.check(lib.afq_propagate_constrained(C.byref(eng.dims), p, C.byref(st),
                                                      fields[s].data_ptr(), w, wb, stream),
                        "afq_propagate_constrained")
         _lib.check(lib.afq_block_end(C.byref(eng.dims), p, C.byref(st), out_row.data_ptr(), w, wb,
                                      stream), "afq_block_end")
+        st.flags = 0  # QR changed the walkers in place
+        note_state(prop_data, st, eng)
 
     def propagate_phaseless(self, ham, ham_data: dict, prop, prop_data: dict, trial, wave_data: dict):
         """sampling.py:343-365.  Returns (E, prop_data) with E a 0-d device tensor."""

@@ -88,7 +88,15 @@ typedef struct afq_state {
   double* overlaps;    /* (W,) complex128                                            */
   double* scalars;     /* device doubles: [0] e_estimate, [1] pop_control_ene_shift,
                           [2] n_killed_walkers (accumulated), [3..7] reserved       */
+  int32_t flags;       /* host-side; AFQ_STATE_GREEN_CURRENT: the workspace already
+                          holds the force-bias operand (Green's function) of these
+                          walkers, left there by the previous afq_propagate_constrained
+                          on the same workspace.  Set on return by that function;
+                          the caller clears it whenever the walkers change otherwise. */
+  int32_t reserved;
 } afq_state;
+
+enum { AFQ_STATE_GREEN_CURRENT = 1 };
 
 /* Library version (major*10000 + minor*100 + patch). */
 int afq_version(void);
