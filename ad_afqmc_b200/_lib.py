@@ -93,6 +93,9 @@ _SIGS = {
     "afq_gemm_split_bf16": ([C.c_void_p * 3, C.c_int, C.c_void_p * 3, C.c_int, C.c_int, C.c_void_p,
                              C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64,
                              C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p], C.c_int),
+    "afq_stochastic_reconfiguration_dev": ([C.POINTER(afq_dims), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "afq_normal_fields_dev": ([C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
+    "afq_uniform_dev": ([C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
     "afq_launch_count": ([C.c_int, C.POINTER(C.c_ulonglong)], C.c_int),
     "afq_profile_begin": ([C.c_int], C.c_int),
     "afq_profile_end": ([C.POINTER(C.c_double), C.POINTER(C.c_int)], C.c_int),

@@ -333,10 +333,9 @@ int afq_orthonormalize(const afq_dims* d, double* const walkers[2], double* norm
   return AFQ_OK;
 }
 
-int afq_stochastic_reconfiguration(const afq_dims* d, const double* weights_in, double zeta,
-                                   int mode, const double* const walkers_in[2],
-                                   double* const walkers_out[2], double* weights_out,
-                                   int32_t* indices, void* stream) {
+static int sr_impl(const afq_dims* d, const double* weights_in, double zeta, const double* zeta_dev,
+                   int mode, const double* const walkers_in[2], double* const walkers_out[2],
+                   double* weights_out, int32_t* indices, void* stream) {
   Layout L;
   int rc = make_layout(d, L);
   if (rc != AFQ_OK) return rc;
@@ -345,7 +344,7 @@ int afq_stochastic_reconfiguration(const afq_dims* d, const double* weights_in, 
   if (L.W > kMaxSrWalkers) return AFQ_ERR_SHAPE;
   if (weights_out == weights_in) return AFQ_ERR_ARG;
   cudaStream_t st = as_stream(stream);
-  AFQ_TRY(launch_sr(L.W, weights_in, zeta, mode, weights_out, indices, st));
+  AFQ_TRY(launch_sr(L.W, weights_in, zeta, zeta_dev, mode, weights_out, indices, st));
   if (walkers_in && walkers_out) {
     for (int s = 0; s < L.ns; ++s) {
       if (!walkers_in[s] || !walkers_out[s]) return AFQ_ERR_NULL;
@@ -355,6 +354,24 @@ int afq_stochastic_reconfiguration(const afq_dims* d, const double* weights_in, 
     }
   }
   return AFQ_OK;
+}
+
+int afq_stochastic_reconfiguration(const afq_dims* d, const double* weights_in, double zeta,
+                                   int mode, const double* const walkers_in[2],
+                                   double* const walkers_out[2], double* weights_out,
+                                   int32_t* indices, void* stream) {
+  return sr_impl(d, weights_in, zeta, nullptr, mode, walkers_in, walkers_out, weights_out, indices,
+                 stream);
+}
+
+int afq_stochastic_reconfiguration_dev(const afq_dims* d, const double* weights_in,
+                                       const double* zeta_dev, int mode,
+                                       const double* const walkers_in[2],
+                                       double* const walkers_out[2], double* weights_out,
+                                       int32_t* indices, void* stream) {
+  if (!zeta_dev) return AFQ_ERR_NULL;
+  return sr_impl(d, weights_in, 0.0, zeta_dev, mode, walkers_in, walkers_out, weights_out,
+                 indices, stream);
 }
 
 int afq_block_end(const afq_dims* d, const void* prepared, afq_state* s, double* block_out,
@@ -373,6 +390,22 @@ int afq_block_end(const afq_dims* d, const void* prepared, afq_state* s, double*
   if (rc != AFQ_OK) return rc;
   AFQ_TRY(launch_ovlp_combine(L.W, L.ns, L.mult, Wk + L.w_wscal, s->overlaps, 2, st));
   AFQ_TRY(launch_block_end(L, Wk, s->weights, s->scalars, d->dt, block_out, st));
+  return AFQ_OK;
+}
+
+int afq_normal_fields_dev(double* out, int64_t n, uint64_t seed, uint64_t* counter,
+                          void* stream) {
+  if (!out || !counter) return AFQ_ERR_NULL;
+  if (n <= 0) return AFQ_ERR_ARG;
+  AFQ_TRY(launch_normal_dev(out, n, seed, reinterpret_cast<unsigned long long*>(counter),
+                            as_stream(stream)));
+  return AFQ_OK;
+}
+
+int afq_uniform_dev(double* out, uint64_t seed, uint64_t* counter, void* stream) {
+  if (!out || !counter) return AFQ_ERR_NULL;
+  AFQ_TRY(launch_uniform_dev(out, seed, reinterpret_cast<unsigned long long*>(counter),
+                             as_stream(stream)));
   return AFQ_OK;
 }
 

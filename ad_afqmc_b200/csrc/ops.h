@@ -58,14 +58,18 @@ cudaError_t launch_qr(const Layout& L, double* const walkers[2], double* norms, 
                       cudaStream_t st);
 // W <= kMaxSrWalkers (cumulative sum kept in shared memory)
 constexpr int kMaxSrWalkers = 16384;
-cudaError_t launch_sr(int W, const double* weights_in, double zeta, int mode,
-                      double* weights_out, int* indices, cudaStream_t st);
+cudaError_t launch_sr(int W, const double* weights_in, double zeta, const double* zeta_dev,
+                      int mode, double* weights_out, int* indices, cudaStream_t st);
 cudaError_t launch_gather(int W, long long walker_doubles, const double* in, double* out,
                           const int* indices, cudaStream_t st);
 cudaError_t launch_block_end(const Layout& L, double* work, const double* weights,
                              double* scalars, double dt, double* block_out, cudaStream_t st);
 cudaError_t launch_normal(double* out, long long n, unsigned long long seed,
                           unsigned long long offset, cudaStream_t st);
+cudaError_t launch_normal_dev(double* out, long long n, unsigned long long seed,
+                              unsigned long long* counter, cudaStream_t st);
+cudaError_t launch_uniform_dev(double* out, unsigned long long seed, unsigned long long* counter,
+                               cudaStream_t st);
 cudaError_t launch_set_scalars(double* dst, double a, double b, double c, double d,
                                cudaStream_t st);
 

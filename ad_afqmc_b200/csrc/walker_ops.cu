@@ -227,9 +227,10 @@ __global__ void qr_norm_kernel(int W, int ns, int restricted, const double* sect
 // comb reconfiguration (single CTA); bit-exact: serial cumsum, explicit
 // round-to-nearest arithmetic in the reference's expression order.
 // ---------------------------------------------------------------------------
-__global__ void sr_kernel(int W, const double* win, double zeta, int mode, double* wout,
-                          int* idx) {
+__global__ void sr_kernel(int W, const double* win, double zeta_host, const double* zeta_dev,
+                          int mode, double* wout, int* idx) {
   extern __shared__ double cum[];
+  const double zeta = zeta_dev ? *zeta_dev : zeta_host;
   if (threadIdx.x == 0) {
     double s = 0.0;
     for (int i = 0; i < W; ++i) {
@@ -339,6 +340,40 @@ __global__ void normal_kernel(double* out, long long n, unsigned long long seed,
   }
 }
 
+// fields from the Philox stream at a device-resident counter; the counter
+// then advances by the pairs consumed (graph replays draw fresh numbers)
+__global__ void normal_dev_kernel(double* out, long long n, unsigned long long seed,
+                                  const unsigned long long* counter) {
+  const long long npair = (n + 1) / 2;
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  const unsigned long long base = *counter;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npair;
+       i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long ctr = base + (unsigned long long)i;
+    const uint4 r = philox10(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), 0u, 0u), key);
+    const double u1 = u53(r.x, r.y), u2 = u53(r.z, r.w);
+    const double rad = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    out[2 * i] = rad * cs;
+    if (2 * i + 1 < n) out[2 * i + 1] = rad * sn;
+  }
+}
+
+// one U(0,1) at the counter (third word of the Philox block: a stream
+// disjoint from the normals), counter advanced by one; then the counter of the
+// normals is advanced by `advance`
+__global__ void uniform_dev_kernel(double* out, unsigned long long seed,
+                                   unsigned long long* counter, unsigned long long advance) {
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  const unsigned long long ctr = *counter;
+  if (out) {
+    const uint4 r = philox10(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), 1u, 0u), key);
+    *out = u53(r.x, r.y);
+  }
+  *counter = ctr + advance;
+}
+
 __global__ void set_scalars_kernel(double* dst, double a, double b, double c, double d) {
   dst[0] = a;
   dst[1] = b;
@@ -380,14 +415,14 @@ cudaError_t launch_qr(const Layout& L, double* const walkers[2], double* norms, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_sr(int W, const double* weights_in, double zeta, int mode,
-                      double* weights_out, int* indices, cudaStream_t st) {
+cudaError_t launch_sr(int W, const double* weights_in, double zeta, const double* zeta_dev,
+                      int mode, double* weights_out, int* indices, cudaStream_t st) {
   const size_t smem = size_t(W) * sizeof(double);
   cudaError_t e =
       cudaFuncSetAttribute(sr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   ProfScope ps(K_SR, st);
-  sr_kernel<<<1, 1024, smem, st>>>(W, weights_in, zeta, mode, weights_out, indices);
+  sr_kernel<<<1, 1024, smem, st>>>(W, weights_in, zeta, zeta_dev, mode, weights_out, indices);
   return cudaGetLastError();
 }
 
@@ -418,6 +453,30 @@ cudaError_t launch_normal(double* out, long long n, unsigned long long seed,
   if (blocks < 1) blocks = 1;
   ProfScope ps(K_NORMAL, st);
   normal_kernel<<<(int)blocks, 256, 0, st>>>(out, n, seed, offset);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_normal_dev(double* out, long long n, unsigned long long seed,
+                              unsigned long long* counter, cudaStream_t st) {
+  const long long npair = (n + 1) / 2;
+  long long blocks = (npair + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  {
+    ProfScope ps(K_NORMAL, st);
+    normal_dev_kernel<<<(int)blocks, 256, 0, st>>>(out, n, seed, counter);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  ProfScope ps(K_MISC, st);
+  uniform_dev_kernel<<<1, 1, 0, st>>>(nullptr, seed, counter, (unsigned long long)npair);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_uniform_dev(double* out, unsigned long long seed, unsigned long long* counter,
+                               cudaStream_t st) {
+  ProfScope ps(K_MISC, st);
+  uniform_dev_kernel<<<1, 1, 0, st>>>(out, seed, counter, 1ull);
   return cudaGetLastError();
 }
 

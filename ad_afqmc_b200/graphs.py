@@ -1,0 +1,161 @@
+"""Energy blocks recorded as CUDA graphs.
+
+``BlockGraph`` records one energy block of the phaseless loop for one walker
+population — the body of ``sampler.propagate_phaseless`` with
+``n_ene_blocks = n_sr_blocks = 1`` (sampling.py:52-94, 146-168, 343-365)
+followed by the driver's ``e_estimate`` update (driver.py:168):
+
+    pop_control_ene_shift = e_estimate ; n_killed = 0
+    fields ~ N(0,1) (S, W, G)                  Philox, device-resident counter
+    S x propagate_constrained                  Green's function reused across steps
+    block end: QR, overlaps, local energies, clamp, block energy, pop-shift EMA
+    zeta ~ U(0,1) ; comb reconfiguration ; overlaps of the new walkers
+    e_estimate = 0.9 e_estimate + 0.1 E_block
+
+Every per-block input lives on the device (RNG counter, zeta, scalars), so a
+replay draws fresh random numbers and needs no host round trip.
+
+``BatchGraph`` records the blocks of many independent solves (fragments of
+different sizes) into ONE graph, each solve on its own forked stream, so a
+single replay advances every fragment by one block and the solves overlap on
+the device.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional
+
+import torch
+
+from . import _lib
+from .propagation import make_state, sync_scalars
+from .walkers import UHFWalkers
+
+
+class BlockGraph:
+    def __init__(self, ham, ham_data, prop, trial, wave_data, prop_data, n_prop_steps: int = 10,
+                 update_estimate: bool = True):
+        self.prop, self.trial, self.wave_data, self.ham_data = prop, trial, wave_data, ham_data
+        self.eng = prop.engine(ham_data, trial, wave_data)
+        if not self.eng.has_prop:
+            raise _lib.AfqError("propagation intermediates missing")
+        self.S = int(n_prop_steps)
+        self.update_estimate = update_estimate
+        self.pd = prop_data
+        sync_scalars(prop_data)
+        w = prop_data["walkers"]
+        self.tensors = list(w.data) if isinstance(w, UHFWalkers) else [w.data]
+        self.tmp = [torch.empty_like(t) for t in self.tensors]
+        dev = self.tensors[0].device
+        W = prop.n_walkers
+        G = int(ham_data["chol"].shape[0])
+        self.fields = torch.empty(self.S, W, G, dtype=torch.float64, device=dev)
+        key = prop_data["key"]
+        self.seed = key.seed
+        self.counter = torch.tensor([key.counter], dtype=torch.int64, device=dev)
+        self.zeta = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.block_out = torch.zeros(2, dtype=torch.float64, device=dev)
+        self.w_tmp = torch.empty_like(prop_data["weights"])
+        self.idx = torch.empty(W, dtype=torch.int32, device=dev)
+        self.small = torch.empty(W * 16, dtype=torch.float64, device=dev)  # own: solves may overlap
+        self.mo = trial._mo_list(wave_data)
+        self.graph: Optional[torch.cuda.CUDAGraph] = None
+        self.launches_per_block = 0
+
+    # -- the recorded body ---------------------------------------------------
+    def body(self) -> None:
+        lib = _lib.lib()
+        stream = _lib.stream_handle()
+        pd, eng = self.pd, self.eng
+        sc = pd["_scalars"]
+        sc[1].copy_(sc[0])  # pop_control_ene_shift = e_estimate
+        sc[2].zero_()       # n_killed_walkers
+        n0 = _lib.launch_count()
+        _lib.check(lib.afq_normal_fields_dev(self.fields.data_ptr(), self.fields.numel(), self.seed,
+                                             self.counter.data_ptr(), stream), "afq_normal_fields_dev")
+        st = make_state(pd)  # GREEN_CURRENT clear: the first step computes G
+        p, w, wb = eng.handle
+        for s in range(self.S):
+            _lib.check(lib.afq_propagate_constrained(C.byref(eng.dims), p, C.byref(st),
+                                                     self.fields[s].data_ptr(), w, wb, stream),
+                       "afq_propagate_constrained")
+        _lib.check(lib.afq_block_end(C.byref(eng.dims), p, C.byref(st), self.block_out.data_ptr(), w,
+                                     wb, stream), "afq_block_end")
+        _lib.check(lib.afq_uniform_dev(self.zeta.data_ptr(), self.seed, self.counter.data_ptr(), stream),
+                   "afq_uniform_dev")
+        win = _lib.pair(*[t.data_ptr() for t in self.tensors] + [None] * (2 - len(self.tensors)))
+        wout = _lib.pair(*[t.data_ptr() for t in self.tmp] + [None] * (2 - len(self.tmp)))
+        _lib.check(lib.afq_stochastic_reconfiguration_dev(
+            C.byref(eng.dims), pd["weights"].data_ptr(), self.zeta.data_ptr(), _lib.AFQ_SR_LOCAL, win, wout,
+            self.w_tmp.data_ptr(), self.idx.data_ptr(), stream), "afq_stochastic_reconfiguration_dev")
+        for t, u in zip(self.tensors, self.tmp):
+            t.copy_(u)
+        pd["weights"].copy_(self.w_tmp)
+        mo = _lib.pair(self.mo[0].data_ptr(), self.mo[-1].data_ptr())
+        _lib.check(lib.afq_calc_overlap(C.byref(eng.dims), mo, win, pd["overlaps"].data_ptr(),
+                                        self.small.data_ptr(), self.small.numel() * 8, stream),
+                   "afq_calc_overlap")
+        sc[2].div_(self.prop.n_walkers)
+        if self.update_estimate:
+            sc[0].mul_(0.9).add_(0.1 * self.block_out[0])
+        self.launches_per_block = _lib.launch_count() - n0
+        pd.pop("_afq_green_of", None)
+
+    # -- capture / replay ----------------------------------------------------
+    def capture(self, warmup: int = 1) -> "BlockGraph":
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(warmup):
+                self.body()
+        torch.cuda.current_stream().wait_stream(s)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.body()
+        return self
+
+    def replay(self) -> torch.Tensor:
+        """One block; returns the block (energy, weight) device tensor."""
+        self.graph.replay()
+        return self.block_out
+
+    @property
+    def e_estimate(self) -> torch.Tensor:
+        return self.pd["_scalars"][0]
+
+
+class BatchGraph:
+    """Blocks of many independent solves in one graph (one forked stream each)."""
+
+    def __init__(self, blocks: List[BlockGraph], n_streams: int = 16):
+        self.blocks = blocks
+        self.n_streams = max(1, min(n_streams, len(blocks)))
+        self.graph: Optional[torch.cuda.CUDAGraph] = None
+
+    def _record(self):
+        main = torch.cuda.current_stream()
+        streams = [torch.cuda.Stream() for _ in range(self.n_streams)]
+        for s in streams:
+            s.wait_stream(main)
+        for i, b in enumerate(self.blocks):
+            with torch.cuda.stream(streams[i % self.n_streams]):
+                b.body()
+        for s in streams:
+            main.wait_stream(s)
+
+    def capture(self, warmup: int = 1) -> "BatchGraph":
+        for _ in range(warmup):
+            self._record()
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._record()
+        return self
+
+    def replay(self) -> None:
+        self.graph.replay()
+
+    @property
+    def launches_per_block(self) -> int:
+        return sum(b.launches_per_block for b in self.blocks)

@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_hi"])
+    ap.add_argument("--eager", action="store_true",
+                    help="launch every kernel from Python instead of replaying the block's CUDA graph")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 comparison leg and the block-energy error check")
     ap.add_argument("--config", default=CONFIG)
@@ -209,29 +211,54 @@ def main():
         pd_["e_estimate"] = 0.9 * pd_["e_estimate"] + 0.1 * e
         return pd_, e
 
-    def timed_run(precision, steps, warmup, profile_kernel=None):
+    def timed_run(precision, steps, warmup, profile_kernel=None, graph=False):
         hd, wv, pr, pd_ = setup(sys_, precision, 1000 + rank)
-        smp_ = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1)
+        if graph:
+            # the block (fields, 10 steps, block end, comb, e_estimate update) as one CUDA graph
+            from ad_afqmc_b200.graphs import BlockGraph
+            bg = BlockGraph(ham, hd, pr, trial, wv, pd_, n_prop_steps=S).capture(warmup=1)
+
+            def run_block():
+                e = bg.replay()[0]
+                if world > 1:
+                    t = torch.stack([e * torch.sum(pd_["weights"]), torch.sum(pd_["weights"])])
+                    dist.all_reduce(t)
+        else:
+            smp_ = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1)
+
+            def run_block():
+                nonlocal pd_
+                pd_, _ = one_block(smp_, hd, wv, pr, pd_)
         for _ in range(warmup):
-            pd_, _ = one_block(smp_, hd, wv, pr, pd_)
+            run_block()
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         n0 = _lib.launch_count()
-        if profile_kernel:
+        if profile_kernel and not graph:
             _lib.profile_begin(profile_kernel)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         start.record()
         for _ in range(steps):
-            pd_, _ = one_block(smp_, hd, wv, pr, pd_)
+            run_block()
         stop.record()
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         ms = start.elapsed_time(stop)
-        kern = _lib.profile_end() if profile_kernel else (0.0, 0)
+        kern = _lib.profile_end() if (profile_kernel and not graph) else (0.0, 0)
         launches = _lib.launch_count() - n0
+        if graph:
+            launches = bg.launches_per_block * steps
+            if profile_kernel:
+                # the dominant kernel timed with CUDA events in eager blocks of the same state
+                smp_ = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1)
+                _lib.profile_begin(profile_kernel)
+                for _ in range(max(1, steps // 2)):
+                    pd_, _ = one_block(smp_, hd, wv, pr, pd_)
+                torch.cuda.synchronize()
+                kern = _lib.profile_end()
         if world > 1:
             t = torch.tensor([ms], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -241,14 +268,14 @@ def main():
     clk_path = os.path.join(tempfile.gettempdir(), f"afq_clocks_{rank}.csv")
     clk = clocks_start(clk_path)
     ms_total, (kern_ms, kern_n), launches, killed, (ham_data, wave, prop, pd) = timed_run(
-        args.precision, args.steps, args.warmup, "vhs")
+        args.precision, args.steps, args.warmup, "vhs", graph=not args.eager)
     clocks = clocks_stop(clk, clk_path, torch.cuda.current_device())
     value = world * W * S * args.steps / (ms_total / 1e3)
 
     # ---- FP64 GPU path on the same workload, and the block-energy error -------
     compare = None
     if not args.no_compare and args.precision != "fp64":
-        ms64, _, _, _, _ = timed_run("fp64", max(2, args.steps // 2), 1)
+        ms64, _, _, _, _ = timed_run("fp64", max(2, args.steps // 2), 1, graph=not args.eager)
         v64 = world * W * S * max(2, args.steps // 2) / (ms64 / 1e3)
         # same-shape system with a surviving population (Cholesky vectors x0.25):
         # identical walkers and device-drawn fields for both precisions
@@ -267,7 +294,13 @@ def main():
             for _ in range(nb):
                 pd_, e = one_block(smp_, hd, wv, pr, pd_)
                 es.append(float(e))
-            energies[precision] = (es, float(pd_["n_killed_walkers"]))
+            # unclamped weighted local energy of the final walkers (stays meaningful
+            # when the sqrt(2/dt) clamp pins the block energies to e_estimate)
+            el = torch.real(trial.calc_energy(pd_["walkers"], hd, wv))
+            wsum = torch.sum(pd_["weights"])
+            e_unclamped = float(torch.sum(el * pd_["weights"]) / wsum) if float(wsum) > 0 else float("nan")
+            clamped = float(torch.mean((torch.abs(el - pd_["e_estimate"]) > (2.0 / dt) ** 0.5).double()))
+            energies[precision] = (es, float(pd_["n_killed_walkers"]), e_unclamped, clamped)
             del hd, pr, pd_
         err = max(abs(a - b) for a, b in zip(energies[args.precision][0], energies["fp64"][0]))
         compare = {"fp64_value": v64, "fp64_ms_per_step": ms64 / max(2, args.steps // 2),
@@ -277,7 +310,9 @@ def main():
                                          "same walkers and fields, vs the FP64 GPU path (which "
                                          "matches the NumPy oracle to 1e-8 Ha)",
                    "block_energies_fp64": energies["fp64"][0],
-                   "killed_fraction_check": energies[args.precision][1]}
+                   "killed_fraction_check": energies[args.precision][1],
+                   "unclamped_local_energy_error_ha": abs(energies[args.precision][2] - energies["fp64"][2]),
+                   "clamped_fraction_check": energies["fp64"][3]}
 
     # ---- end to end through the public API with host buffers -------------
     e2e = None
@@ -360,7 +395,8 @@ def main():
                       "n_walkers_per_gpu": W, "n_prop_steps_per_bench_step": S, "dt": dt,
                       "precision": args.precision, "parallelism": f"replicas x{world}",
                       "l2": "working set (VHS 328 MB, chol 320 MB) exceeds the 126 MB L2",
-                      "chol_scale": args.chol_scale, "killed_walker_fraction": killed},
+                      "chol_scale": args.chol_scale, "killed_walker_fraction": killed,
+                      "launch": "eager" if args.eager else "cuda_graph_per_block"},
            "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
            "clocks": clocks, "compare": compare}
     print(json.dumps(out))

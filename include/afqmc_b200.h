@@ -188,6 +188,15 @@ int afq_stochastic_reconfiguration(const afq_dims* d, const double* weights_in, 
                                    double* const walkers_out[2], double* weights_out,
                                    int32_t* indices, void* stream);
 
+/* As afq_stochastic_reconfiguration with zeta read from device memory, so
+ * that the call can be recorded in a CUDA graph and replayed with fresh
+ * uniforms (see afq_uniform_dev). */
+int afq_stochastic_reconfiguration_dev(const afq_dims* d, const double* weights_in,
+                                       const double* zeta_dev, int mode,
+                                       const double* const walkers_in[2],
+                                       double* const walkers_out[2], double* weights_out,
+                                       int32_t* indices, void* stream);
+
 /* Block end of sampler._block_scan (sampling.py:76-94): killed-walker count,
  * QR, overlaps, local energies with the sqrt(2/dt) clamp, block energy and
  * weight, and the population-control shift update.
@@ -200,6 +209,13 @@ int afq_block_end(const afq_dims* d, const void* prepared, afq_state* s, double*
  * Replaces random.normal(subkey, (S, W, G)) in sampler._block_scan
  * (sampling.py:63-71); the bits differ from JAX threefry by design. */
 int afq_normal_fields(double* out, int64_t n, uint64_t seed, uint64_t offset, void* stream);
+
+/* Graph-replayable variants: the Philox counter lives in device memory
+ * (*counter) and advances by the draws consumed, so a captured CUDA graph
+ * draws fresh fields/uniforms on every replay.  afq_uniform_dev writes one
+ * U(0,1) (for the reconfiguration comb) to *out. */
+int afq_normal_fields_dev(double* out, int64_t n, uint64_t seed, uint64_t* counter, void* stream);
+int afq_uniform_dev(double* out, uint64_t seed, uint64_t* counter, void* stream);
 
 /* Split x (n,) float64 into npieces (1..3) bfloat16 arrays with
  * x ~= p0 + p1 (+ p2), each piece rounded to nearest from the remainder.

@@ -274,3 +274,29 @@ def test_config_rhf_n200_subset_parity_and_permutation():
     perm = np.array([2, 0, 3, 1])
     e_p = _np(d_trial.calc_energy(RHFWalkers(walkers[perm].copy()), d_ham, d_wave))
     assert np.array_equal(e_p, e_d[perm])
+
+
+def test_config_uhf_n300_subset_parity():
+    """Config-3 shapes (N=300, Na=60, Nb=58, G=1500): measurements and one step
+    on a few walkers (QR and walkers take the in-place global-memory paths)."""
+    from ad_afqmc_b200.walkers import UHFWalkers
+
+    sys_ = make_system(300, (60, 58), 1500, seed=1003, trial="uhf", chol_scale=0.25)
+    rng = np.random.default_rng(9)
+    W = 3
+    walkers = [near_trial_walkers(rng, sys_.mo_coeff[0], W, eps=0.05),
+               near_trial_walkers(rng, sys_.mo_coeff[1], W, eps=0.05)]
+    o_trial, o_ham, o_wave, o_prop = oracle_system(sys_, "unrestricted", 0.005)
+    d_trial, d_ham, d_wave, d_prop, _ = device_system(sys_, "unrestricted", 0.005, W)
+    dw = UHFWalkers([walkers[0].copy(), walkers[1].copy()])
+    e_d = _np(d_trial.calc_energy(dw, d_ham, d_wave))
+    assert np.max(np.abs(e_d - o_trial.calc_energy(walkers, o_ham, o_wave))) < 1e-8
+    fields = rng.standard_normal((W, 1500))
+    o_prop.n_walkers = W
+    o_pd = o_prop.init_prop_data(o_trial, o_wave, o_ham, init_walkers=copy.deepcopy(walkers))
+    o_pd = o_prop.propagate_constrained(o_trial, o_ham, o_pd, fields, o_wave)
+    d_pd = d_prop.init_prop_data(d_trial, d_wave, d_ham, 0, init_walkers=dw)
+    d_pd = d_prop.propagate_constrained(d_trial, d_ham, d_pd, fields, d_wave)
+    for s in range(2):
+        assert rel_err(_np(d_pd["walkers"].data[s]), o_pd["walkers"][s]) < 1e-10
+    assert np.allclose(_np(d_pd["weights"]), o_pd["weights"], rtol=1e-10, atol=1e-13)
