@@ -99,18 +99,18 @@ int energy_impl(const Layout& L, const double* prep, double* work, const double*
   GreenArgs a = green_args(L, prep, work, walkers);
   for (int s = 0; s < L.ns; ++s) {
     a.sec[s].rh1 = prep + L.p_rh1[s];
-    if (L.mixed)
-      piece_ptrs(work, L.v_gt[s], L.v_gt_ps[s], L.npc, a.sec[s].gtb);
-    else
+    if (L.exch_f64[s])
       a.sec[s].theta = work + L.w_theta[s];
+    else
+      piece_ptrs(work, L.v_gt[s], L.v_gt_ps[s], L.npc, a.sec[s].gtb);
   }
   AFQ_TRY(launch_green(a, st));
   for (int s = 0; s < L.ns; ++s) {
-    if (L.mixed) {
+    if (L.exch_f64[s]) {
+      AFQ_TRY(launch_exchange(L, prep, work, s, st));
+    } else {
       const int rc = mixed_exchange(L, prep, work, s, st);
       if (rc != AFQ_OK) return rc;
-    } else {
-      AFQ_TRY(launch_exchange(L, prep, work, s, st));
     }
   }
   AFQ_TRY(launch_energy_combine(L, prep, work, eout, eout_stride, st));

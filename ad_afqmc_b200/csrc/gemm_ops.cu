@@ -27,6 +27,7 @@ using CfgP80 = F64Cfg<5, 5, 1, 2>;   // 40 x 80,  2 warps
 using CfgP120 = F64Cfg<5, 5, 1, 3>;  // 40 x 120, 3 warps
 using CfgX80 = F64Cfg<5, 5, 3, 2>;   // 120 x 80,  6 warps (exchange)
 using CfgX120 = F64Cfg<5, 5, 3, 3>;  // 120 x 120, 9 warps (exchange)
+using CfgX160 = F64Cfg<4, 5, 4, 4>;  // 128 x 160, 16 warps (exchange, No > 60)
 
 template <class Cfg>
 cudaError_t set_smem(const void* fn, size_t bytes) {
@@ -443,7 +444,9 @@ static cudaError_t run_exch(const Layout& L, const double* prep, double* work, i
 cudaError_t launch_exchange(const Layout& L, const double* prep, double* work, int s,
                             cudaStream_t st) {
   if (L.ex[s].bn == 80) return run_exch<CfgX80>(L, prep, work, s, st);
-  return run_exch<CfgX120>(L, prep, work, s, st);
+  if (L.ex[s].bn == 120) return run_exch<CfgX120>(L, prep, work, s, st);
+  if (L.ex[s].bn == 160) return run_exch<CfgX160>(L, prep, work, s, st);
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_energy_combine(const Layout& L, const double* prep, double* work, double* eout,

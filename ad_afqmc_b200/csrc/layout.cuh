@@ -10,15 +10,16 @@
 
 namespace afq {
 
-constexpr int kMaxOcc = 60;  // largest occupied block per spin accepted by the kernels
+constexpr int kMaxOcc = 64;  // largest occupied block per spin accepted by the kernels
 
 inline long long round_even(long long x) { return (x + 1) & ~1LL; }
 inline long long align_up(long long x, long long a) { return (x + a - 1) / a * a; }
 
 // Exchange-energy tile choice (see exchange kernel): gpt Cholesky vectors
-// per 120-row tile and wpt walkers per BN-column tile.
+// per BM-row tile and wpt walkers per BN-column tile.
 struct ExchTile {
-  int bn;   // 80 or 120
+  int bm;   // 120 or 128
+  int bn;   // 80, 120 or 160
   int gpt;  // Cholesky vectors per tile
   int wpt;  // walkers per tile
   int mt;   // number of row tiles = ceil(G / gpt)
@@ -63,6 +64,7 @@ struct Layout {
   int mixed, npc;      // tensor-core path and bf16 pieces per operand (2 or 3)
   long long Kb, Gb, Nb, Kv;  // bf16 row strides (multiples of 8 elements)
   UExchTile uex[2];
+  int exch_f64[2];     // exchange of this spin on the FP64 kernel (always when !mixed)
   // bf16 buffers, offsets in doubles (4 bf16 per double); [piece] stride given by *_ps
   long long q_rccat, q_cholT, q_exph1[2], q_rc[2];
   long long q_rccat_ps, q_cholT_ps, q_exph1_ps, q_rc_ps[2];
@@ -79,19 +81,21 @@ struct Layout {
 };
 
 inline ExchTile choose_exch_tile(int no, int G, int W) {
-  ExchTile best{80, 1, 1, G};
+  // (BM, BN) of the FP64 exchange kernels: 120 x 80, 120 x 120, 128 x 160
+  const int bms[3] = {120, 120, 128}, bns[3] = {80, 120, 160};
+  ExchTile best{0, 0, 0, 0, 0};
   double best_eff = -1.0;
-  const int bns[2] = {80, 120};
-  for (int i = 0; i < 2; ++i) {
-    const int bn = bns[i];
-    if (2 * no > bn || no > 120) continue;
-    const int gpt = 120 / no, wpt = bn / (2 * no);
-    const double eff = double(gpt * no) / 120.0 * double(wpt * 2 * no) / double(bn);
+  for (int i = 0; i < 3; ++i) {
+    const int bm = bms[i], bn = bns[i];
+    if (2 * no > bn || no > bm) continue;
+    const int gpt = bm / no, wpt = bn / (2 * no);
+    const double eff = double(gpt * no) / bm * double(wpt * 2 * no) / double(bn);
     if (eff > best_eff + 1e-9) {
       best_eff = eff;
-      best = ExchTile{bn, gpt, wpt, (G + gpt - 1) / gpt};
+      best = ExchTile{bm, bn, gpt, wpt, (G + gpt - 1) / gpt};
     }
   }
+  (void)W;
   return best;
 }
 
@@ -145,11 +149,13 @@ inline int make_layout(const afq_dims* d, Layout& L) {
   L.Nb = round8(L.N);
   L.Kv = round8(2LL * L.N);
   for (int s = 0; s < 2; ++s) L.uex[s] = choose_uexch_tile(L.no[s], L.G, L.npc);
-  if (L.mixed) {  // the exchange partial sums follow the tensor-core tiling
-    for (int s = 0; s < L.ns; ++s) {
-      if (L.uex[s].bn == 0) return AFQ_ERR_SHAPE;  // no tile fits shared memory
-      L.ex[s].mt = L.uex[s].mt;
-    }
+  for (int s = 0; s < 2; ++s) {
+    if (L.ex[s].bn == 0) return AFQ_ERR_SHAPE;
+    // three-piece operands of a large occupied block leave no room for two
+    // pipeline stages of the tensor-core exchange: that spin's exchange runs
+    // on the FP64 kernel (exact) instead
+    L.exch_f64[s] = !L.mixed || L.uex[s].bn == 0;
+    if (!L.exch_f64[s]) L.ex[s].mt = L.uex[s].mt;  // partial sums follow the tensor-core tiling
   }
 
   // ---- prepared buffer

@@ -103,7 +103,21 @@ class BlockGraph:
         pd.pop("_afq_green_of", None)
 
     # -- capture / replay ----------------------------------------------------
-    def capture(self, warmup: int = 1) -> "BlockGraph":
+    def capture(self, warmup: int = 1, device_sync: bool = True) -> "BlockGraph":
+        """Record the block.  With device_sync=False the capture runs on the
+        current (non-default) stream without synchronising the device, so
+        other streams keep running (used when admitting solves while others
+        are in flight)."""
+        if not device_sync:
+            for _ in range(warmup):
+                self.body()
+            self.graph = torch.cuda.CUDAGraph()
+            self.graph.capture_begin(capture_error_mode="thread_local")
+            try:
+                self.body()
+            finally:
+                self.graph.capture_end()
+            return self
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):

@@ -52,7 +52,7 @@ def test_sizes_scale_with_shape():
 
 
 @pytest.mark.parametrize("kw,code", [
-    (dict(norb=0), 1), (dict(nocc=(0, 0)), 1), (dict(nocc=(61, 61), norb=80), 1),
+    (dict(norb=0), 1), (dict(nocc=(0, 0)), 1), (dict(nocc=(65, 65), norb=80), 1),
     (dict(nocc=(5, 4), walker_type=1), 1),                   # rhf needs Na == Nb
     (dict(walker_type=0, trial_type=1, nocc=(5, 4)), 1),     # uhf trial + restricted walkers
     (dict(walker_type=3), 6), (dict(precision=7), 6), (dict(n_exp_terms=0), 6),

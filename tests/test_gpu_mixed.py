@@ -43,6 +43,7 @@ CASES = [
     (64, (16, 16), 300, "rhf", "restricted", 40),
     (48, (13, 11), 200, "uhf", "unrestricted", 24),
     (200, (40, 40), 1000, "rhf", "restricted", 8),
+    (80, (62, 62), 200, "rhf", "restricted", 4),
 ]
 # BF16x6 is limited by FP32 accumulation over K (up to 8000 in the force bias)
 TOL = {"mixed": 1e-4, "mixed_hi": 2e-5}
