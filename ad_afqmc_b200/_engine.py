@@ -9,8 +9,10 @@ from.  Rebuilding intermediates (``hamiltonian.build_*``) drops the cache.
 from __future__ import annotations
 
 import ctypes as C
+import warnings
 from typing import Dict, Optional, Tuple
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -39,6 +41,13 @@ def to_dev(x, dtype=torch.float64) -> torch.Tensor:
         if not t.is_cuda:
             t = t.to(device())
         return t.contiguous()
+    if isinstance(x, np.ndarray) and not x.flags.writeable:
+        # a shared read-only host array: wrap without copying, then one host-to-device copy
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", UserWarning)
+            t = torch.from_numpy(np.ascontiguousarray(x))
+        # asynchronous from page-locked memory (the owner keeps it alive and unchanged)
+        return t.to(device=device(), dtype=dtype, non_blocking=t.is_pinned()).contiguous()
     return torch.as_tensor(x, dtype=dtype, device=device()).contiguous()
 
 

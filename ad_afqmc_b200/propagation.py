@@ -160,7 +160,12 @@ class propagator_afqmc(propagator):
         if "e_estimate" in ham_data:
             pd["e_estimate"] = _scalar(ham_data["e_estimate"])
         else:
-            e = torch.real(trial.calc_energy(pd["walkers"], ham_data, wave_data))
+            if self.precision != "fp64" and "exp_h1" in ham_data:
+                # the propagator's own engine: no FP64 layout built for one energy evaluation
+                e = torch.real(trial.calc_energy(pd["walkers"], ham_data, wave_data,
+                                                 engine=self.engine(ham_data, trial, wave_data)))
+            else:
+                e = torch.real(trial.calc_energy(pd["walkers"], ham_data, wave_data))
             pd["e_estimate"] = torch.sum(e) / self.n_walkers
         pd["pop_control_ene_shift"] = pd["e_estimate"].clone()
         pd["n_killed_walkers"] = 0.0

@@ -114,9 +114,13 @@ class wave_function:
         )
         return out
 
-    def calc_energy(self, walkers: walker_batch, ham_data: dict, wave_data: dict) -> torch.Tensor:
-        """Local energy (W,) complex128 (wavefunctions.py:264-394)."""
-        eng = get_engine(ham_data, self, wave_data, _walker_type(walkers), walkers.n_walkers)
+    def calc_energy(self, walkers: walker_batch, ham_data: dict, wave_data: dict, *,
+                    engine=None) -> torch.Tensor:
+        """Local energy (W,) complex128 (wavefunctions.py:264-394).  ``engine``
+        (keyword only) evaluates it on an existing engine, e.g. the propagator's,
+        instead of the FP64 engine of this shape."""
+        eng = engine if engine is not None else get_engine(ham_data, self, wave_data, _walker_type(walkers),
+                                                           walkers.n_walkers)
         W = walkers.n_walkers
         out = torch.empty(W, dtype=torch.complex128, device=eng.prepared.device)
         p, w, wb = eng.handle

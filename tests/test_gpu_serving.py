@@ -26,11 +26,15 @@ def test_results_identical_alone_and_in_the_mix(precision):
     from ad_afqmc_b200.serving import Server
 
     reqs = _requests()
-    srv = Server(precision, n_prop_steps=4, min_blocks=3, max_blocks=5, target_error=-1.0)
+    # the mix: set up on the worker thread while other solves run
+    srv = Server(precision, n_prop_steps=4, n_eql=2, max_blocks=5, target_error=-1.0)
     mixed = {r.rid: r for r in srv.run(reqs, realtime=False)}
     assert sorted(mixed) == [0, 1, 2, 3]
+    # alone: one slot, set up inline
+    one = Server(precision, max_slots=1, n_prop_steps=4, n_eql=2, max_blocks=5, target_error=-1.0,
+                 setup_thread=False)
     for req in reqs:
-        alone = srv.run([req], realtime=False)[0]
+        alone = one.run([req], realtime=False)[0]
         assert alone.block_energies == mixed[req.rid].block_energies
         assert alone.n_blocks == 5
 
@@ -41,9 +45,23 @@ def test_admission_respects_memory_budget():
     reqs = _requests()
     fp = max(footprint_bytes(r, "mixed") for r in reqs)
     # room for about two solves at a time: all still complete, in arrival order of admission
-    srv = Server("mixed", hbm_budget_gb=2.5 * fp / 1e9, n_prop_steps=3, min_blocks=2, max_blocks=3,
+    srv = Server("mixed", hbm_budget_gb=2.5 * fp / 1e9, n_prop_steps=3, n_eql=1, max_blocks=3,
                  target_error=-1.0)
     res = srv.run(reqs, realtime=False)
     assert len(res) == 4
     admitted = sorted(res, key=lambda r: r.admitted)
     assert [r.rid for r in admitted] == [0, 1, 2, 3]
+
+
+def test_stop_rule_ends_converged_solves_early():
+    """With a loose target every solve stops at the first SEM check (block
+    index max_blocks // 5 = 6 > 4, i.e. after 7 blocks); the blocking rule
+    stops after min_blocks."""
+    from ad_afqmc_b200.serving import Server
+
+    reqs = _requests()[:2]
+    res = Server("mixed", n_prop_steps=3, n_eql=1, max_blocks=30, target_error=10.0).run(reqs, realtime=False)
+    assert all(r.converged and r.n_blocks == 7 for r in res)
+    res = Server("mixed", n_prop_steps=3, n_eql=1, max_blocks=30, target_error=10.0, stop_rule="blocking",
+                 min_blocks=5).run(reqs, realtime=False)
+    assert all(r.converged and r.n_blocks == 5 for r in res)
