@@ -137,6 +137,18 @@ class Engine:
         torch.cuda.current_stream().synchronize()
         self._keep = []
 
+    def ensure_workspace(self) -> None:
+        """Grow the workspace if the shape's tuning record now needs more (the
+        buffers that persist across calls keep their offsets, so a grown
+        workspace only needs the zeroed error flag, which a fresh buffer has).
+        Call it before capturing graphs that use this engine."""
+        _, wbytes = _lib.sizes(self.dims)
+        if wbytes > self.work.numel() * 8:
+            new = torch.zeros(wbytes // 8, dtype=torch.float64, device=self.work.device)
+            new[: self.work.numel()].copy_(self.work)
+            self.work = new
+        self.work_bytes = self.work.numel() * 8
+
     @property
     def handle(self) -> Tuple[int, int, int]:
         return self.prepared.data_ptr(), self.work.data_ptr(), self.work_bytes

@@ -66,6 +66,32 @@ class afq_state(C.Structure):
 AFQ_STATE_GREEN_CURRENT = 1
 
 
+class afq_tuning(C.Structure):
+    """Tile/schedule record of one problem shape (0 = built-in heuristic)."""
+    _fields_ = [
+        ("fb_splitk", C.c_int32),
+        ("fb_bn", C.c_int32),
+        ("vhs_bn", C.c_int32),
+        ("exch_bn", C.c_int32),
+        ("f64_exch_bn", C.c_int32),
+        ("max_stages", C.c_int32),
+        ("grid_cap", C.c_int32),
+        ("reserved", C.c_int32 * 9),
+    ]
+
+    KNOBS = ("fb_splitk", "fb_bn", "vhs_bn", "exch_bn", "f64_exch_bn", "max_stages", "grid_cap")
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k in self.KNOBS}
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "afq_tuning":
+        t = cls()
+        for k, v in d.items():
+            setattr(t, k, int(v))
+        return t
+
+
 class AfqError(RuntimeError):
     pass
 
@@ -96,6 +122,8 @@ _SIGS = {
     "afq_stochastic_reconfiguration_dev": ([C.POINTER(afq_dims), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "afq_normal_fields_dev": ([C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
     "afq_uniform_dev": ([C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
+    "afq_set_tuning": ([C.POINTER(afq_dims), C.c_void_p], C.c_int),
+    "afq_get_tuning": ([C.POINTER(afq_dims), C.POINTER(afq_tuning)], C.c_int),
     "afq_launch_count": ([C.c_int, C.POINTER(C.c_ulonglong)], C.c_int),
     "afq_profile_begin": ([C.c_int], C.c_int),
     "afq_profile_end": ([C.POINTER(C.c_double), C.POINTER(C.c_int)], C.c_int),
@@ -234,6 +262,18 @@ def make_dims(norb, nocc, nchol, nwalkers, walker_type, trial_type, n_exp_terms,
     d.reserved = 0
     d.dt = float(dt)
     return d
+
+
+def set_tuning(d: afq_dims, t: Optional[afq_tuning]) -> None:
+    """Register `t` for every call with dims equal to `d` (None removes it)."""
+    check(lib().afq_set_tuning(C.byref(d), C.cast(C.byref(t), C.c_void_p) if t is not None else None),
+          "afq_set_tuning")
+
+
+def get_tuning(d: afq_dims) -> afq_tuning:
+    t = afq_tuning()
+    check(lib().afq_get_tuning(C.byref(d), C.byref(t)), "afq_get_tuning")
+    return t
 
 
 def sizes(d: afq_dims):

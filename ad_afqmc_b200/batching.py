@@ -41,10 +41,16 @@ def make_fragment_block(spec: Dict, precision: str = "mixed", n_prop_steps: int 
 
 class FragmentBatch:
     def __init__(self, specs: List[Dict], precision: str = "mixed", n_prop_steps: int = 10,
-                 n_streams: int = 16, chol_scale: float = 0.25):
+                 n_streams: int = 16, chol_scale: float = 0.25, tuner=None):
         self.specs = specs
         self.blocks = [make_fragment_block(s, precision, n_prop_steps, chol_scale=chol_scale)
                        for s in specs]
+        self.tuning: List[Optional[Dict]] = [None] * len(self.blocks)
+        if tuner is not None:
+            # per-shape tile records, timed (or read from the cache) before any capture
+            for i, b in enumerate(self.blocks):
+                self.tuning[i] = tuner.tune(b.eng, b.pd)
+            tuner.save()
         self.walker_steps_per_block = sum(s["n_walkers"] for s in specs) * n_prop_steps
         self.batch = BatchGraph(self.blocks, n_streams=n_streams)
 
@@ -71,7 +77,8 @@ def _time(fn, reps: int) -> float:
 
 
 def bench(n_fragments: int = 64, precision: str = "mixed", n_prop_steps: int = 10,
-          n_streams: int = 16, reps: int = 3, seed: int = 1004) -> Dict:
+          n_streams: int = 16, reps: int = 3, seed: int = 1004, tune: bool = False,
+          tuning_cache: Optional[str] = None) -> Dict:
     specs = make_fragment_batch(n_fragments, seed=seed)
     t0 = time.perf_counter()
     fb = FragmentBatch(specs, precision, n_prop_steps, n_streams)
@@ -88,7 +95,26 @@ def bench(n_fragments: int = 64, precision: str = "mixed", n_prop_steps: int = 1
     # all fragments in one graph on forked streams
     fb.capture()
     ms_batch = _time(fb.step, reps)
-    return {
+    extra: Dict = {}
+    if tune:
+        from .autotune import Autotuner, tune_batch
+
+        tuner = Autotuner(cache_path=tuning_cache)
+        t0 = time.perf_counter()
+        recs = [tuner.tune(b.eng, b.pd) for b in fb.blocks]
+        tuner.save()
+        extra["tune_s"] = time.perf_counter() - t0
+        extra["tuned_shapes_changed"] = sum(1 for r in recs if r["tuning"])
+        extra["tuned_fragment_gain"] = sum(r["ms_default"] for r in recs) / sum(r["ms"] for r in recs)
+        fb.capture()
+        extra["batched_graph_tuned_ms"] = _time(fb.step, reps)
+        sched = tune_batch(lambda ns: FragmentBatch(specs, precision, n_prop_steps, ns), tuner,
+                           n_streams=(n_streams, 2 * n_streams), reps=reps)
+        extra["schedule"] = {k: sched[k] for k in ("n_streams", "grid_cap", "ms")}
+        extra["schedule_sweep"] = sched["sweep"]
+        best = min(ms_batch, extra["batched_graph_tuned_ms"], sched["ms"])
+        extra["walker_steps_per_s_tuned"] = ws / (best / 1e3)
+    return extra | {
         "workload": f"{n_fragments} fragments N~U[30,160], No=round(N/4), G~U[4N,6N], W~U[64,256]",
         "precision": precision, "n_streams": n_streams, "walker_steps_per_block": ws,
         "setup_s": setup_s,
@@ -106,9 +132,12 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_hi"])
     ap.add_argument("--streams", type=int, default=16)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--tune", action="store_true", help="autotune tiles per shape and the batch schedule")
+    ap.add_argument("--tuning-cache", default=None)
     a = ap.parse_args()
     torch.cuda.set_device(0)
-    print(json.dumps(bench(a.fragments, a.precision, n_streams=a.streams, reps=a.reps)))
+    print(json.dumps(bench(a.fragments, a.precision, n_streams=a.streams, reps=a.reps, tune=a.tune,
+                           tuning_cache=a.tuning_cache)))
 
 
 if __name__ == "__main__":

@@ -137,6 +137,33 @@ const char* afq_status_string(int status) {
   }
 }
 
+int afq_set_tuning(const afq_dims* d, const afq_tuning* t) {
+  if (!d) return AFQ_ERR_NULL;
+  if (t) {
+    Layout L;
+    const int rc = make_layout(d, L, t);
+    if (rc != AFQ_OK) return rc;
+  }
+  tuning_store(*d, t);
+  return AFQ_OK;
+}
+
+int afq_get_tuning(const afq_dims* d, afq_tuning* out) {
+  if (!out) return AFQ_ERR_NULL;
+  Layout L;
+  const int rc = make_layout(d, L);
+  if (rc != AFQ_OK) return rc;
+  *out = L.tune;
+  out->fb_splitk = L.splitk;
+  out->fb_bn = L.fb_bn;
+  out->vhs_bn = L.vhs_bn;
+  out->exch_bn = L.mixed && !L.exch_f64[0] ? L.uex[0].bn : 0;
+  out->f64_exch_bn = L.ex[0].bn;
+  out->max_stages = L.tune.max_stages;  // 0: as many as fit, per GEMM
+  out->grid_cap = L.tune.grid_cap;      // 0: one CTA per SM
+  return AFQ_OK;
+}
+
 int afq_prepared_size(const afq_dims* d, size_t* bytes) {
   Layout L;
   int rc = make_layout(d, L);

@@ -12,6 +12,10 @@ namespace afq {
 
 constexpr int kMaxOcc = 64;  // largest occupied block per spin accepted by the kernels
 
+// registry of afq_tuning records (tuning.cu)
+bool tuning_lookup(const afq_dims& d, afq_tuning& out);
+void tuning_store(const afq_dims& d, const afq_tuning* t);
+
 inline long long round_even(long long x) { return (x + 1) & ~1LL; }
 inline long long align_up(long long x, long long a) { return (x + a - 1) / a * a; }
 
@@ -56,6 +60,21 @@ inline UExchTile choose_uexch_tile(int no, int G, int npc) {
   return t;
 }
 
+// The exchange tile of one column width, or bn = 0 when it cannot hold a
+// walker or does not fit shared memory (same rules as choose_uexch_tile).
+inline UExchTile uexch_tile_for(int no, int G, int npc, int bn) {
+  UExchTile t{0, 128 / no, 0, 0};
+  const long long budget = 227 * 1024 - 1024 - 256;
+  const long long extra = ((128LL * (2 * no + 2) * 4 + 31) & ~31LL) + 128 * 32 + 128 * 16;
+  const long long stage = (long long)npc * (128 * 128 + bn * 128);
+  if (((2 * no + 15) & ~15) <= bn && 2 * stage + extra <= budget) {
+    t.bn = bn;
+    t.wpt = bn / (2 * no);
+  }
+  t.mt = (G + t.gpt - 1) / t.gpt;
+  return t;
+}
+
 inline long long round8(long long x) { return (x + 7) & ~7LL; }
 
 struct Layout {
@@ -65,6 +84,8 @@ struct Layout {
   long long Kb, Gb, Nb, Kv;  // bf16 row strides (multiples of 8 elements)
   UExchTile uex[2];
   int exch_f64[2];     // exchange of this spin on the FP64 kernel (always when !mixed)
+  afq_tuning tune;     // registered record for this shape (zeros: heuristics)
+  int fb_bn, vhs_bn;   // tensor-core column tiles of the force bias and VHS
   // bf16 buffers, offsets in doubles (4 bf16 per double); [piece] stride given by *_ps
   long long q_rccat, q_cholT, q_exph1[2], q_rc[2];
   long long q_rccat_ps, q_cholT_ps, q_exph1_ps, q_rc_ps[2];
@@ -99,8 +120,16 @@ inline ExchTile choose_exch_tile(int no, int G, int W) {
   return best;
 }
 
+inline ExchTile exch_tile_for(int no, int G, int bn) {
+  const int bm = bn == 160 ? 128 : 120;
+  if ((bn != 80 && bn != 120 && bn != 160) || 2 * no > bn || no > bm) return ExchTile{0, 0, 0, 0, 0};
+  const int gpt = bm / no;
+  return ExchTile{bm, bn, gpt, bn / (2 * no), (G + gpt - 1) / gpt};
+}
+
 // Returns AFQ_OK and fills L, or a shape error.
-inline int make_layout(const afq_dims* d, Layout& L) {
+// `record` (optional) replaces the registered tuning record of this shape.
+inline int make_layout(const afq_dims* d, Layout& L, const afq_tuning* record = nullptr) {
   if (!d) return AFQ_ERR_NULL;
   if (d->norb <= 0 || d->nchol <= 0 || d->nwalkers <= 0) return AFQ_ERR_SHAPE;
   if (d->walker_type != AFQ_RESTRICTED && d->walker_type != AFQ_UNRESTRICTED) return AFQ_ERR_ARG;
@@ -141,16 +170,39 @@ inline int make_layout(const afq_dims* d, Layout& L) {
     while (tiles * sk < 296 && sk < 8 && L.Kfb / (sk * 2) >= 256) sk *= 2;
     L.splitk = sk;
   }
-  for (int s = 0; s < 2; ++s) L.ex[s] = choose_exch_tile(L.no[s], L.G, L.W);
+  if (record)
+    L.tune = *record;
+  else if (!tuning_lookup(*d, L.tune))
+    L.tune = afq_tuning{};
+  const afq_tuning& T = L.tune;
+  if (T.fb_splitk < 0 || T.fb_splitk > 8 || T.max_stages < 0 || T.max_stages == 1 ||
+      T.max_stages > 8 || T.grid_cap < 0)
+    return AFQ_ERR_ARG;
+  if (T.fb_bn != 0 && T.fb_bn != 64 && T.fb_bn != 128) return AFQ_ERR_ARG;
+  if (T.vhs_bn != 0 && T.vhs_bn != 64 && T.vhs_bn != 128) return AFQ_ERR_ARG;
+  if (T.fb_splitk > 0) L.splitk = T.fb_splitk;
+  for (int s = 0; s < 2; ++s) {
+    L.ex[s] = T.f64_exch_bn ? exch_tile_for(L.no[s], L.G, T.f64_exch_bn)
+                            : choose_exch_tile(L.no[s], L.G, L.W);
+    if (T.f64_exch_bn && L.ex[s].bn == 0 && s < L.ns) return AFQ_ERR_ARG;
+  }
   L.mixed = d->precision != AFQ_FP64;
   L.npc = d->precision == AFQ_MIXED_HI ? 3 : 2;
   L.Kb = round8(L.Kfb_used);
   L.Gb = round8(L.G);
   L.Nb = round8(L.N);
   L.Kv = round8(2LL * L.N);
-  for (int s = 0; s < 2; ++s) L.uex[s] = choose_uexch_tile(L.no[s], L.G, L.npc);
+  L.fb_bn = T.fb_bn ? T.fb_bn : 128;
+  L.vhs_bn = T.vhs_bn ? T.vhs_bn : (L.npc == 2 ? 128 : 64);
   for (int s = 0; s < 2; ++s) {
-    if (L.ex[s].bn == 0) return AFQ_ERR_SHAPE;
+    L.uex[s] = choose_uexch_tile(L.no[s], L.G, L.npc);
+    if (T.exch_bn && L.mixed && s < L.ns) {
+      L.uex[s] = uexch_tile_for(L.no[s], L.G, L.npc, T.exch_bn);
+      if (L.uex[s].bn == 0) return AFQ_ERR_ARG;
+    }
+  }
+  for (int s = 0; s < 2; ++s) {
+    if (L.ex[s].bn == 0 && s < L.ns) return AFQ_ERR_SHAPE;
     // three-piece operands of a large occupied block leave no room for two
     // pipeline stages of the tensor-core exchange: that spin's exchange runs
     // on the FP64 kernel (exact) instead
@@ -209,7 +261,6 @@ inline int make_layout(const afq_dims* d, Layout& L) {
   L.w_gpl = take(W * 2 * L.Kfb);
   for (int s = 0; s < 2; ++s) L.w_theta[s] = -1;
   for (int s = 0; s < L.ns; ++s) L.w_theta[s] = take(W * N * 2 * L.no[s]);
-  L.w_fbpart = take((long long)L.splitk * 2 * W * L.Gpad);
   L.w_xt = take(2 * W * L.Gpad);
   L.w_wscal = take(W * 16);
   L.w_vhs = take(W * N * 2 * L.Npad);
@@ -219,10 +270,7 @@ inline int make_layout(const afq_dims* d, Layout& L) {
   L.w_ta = take(pb);
   L.w_tb = take(pb);
   for (int s = 0; s < 2; ++s) L.w_c[s] = L.w_exc[s] = -1;
-  for (int s = 0; s < L.ns; ++s) {
-    L.w_c[s] = take(W * L.G * 2);
-    L.w_exc[s] = take((long long)L.ex[s].mt * W * 2);
-  }
+  for (int s = 0; s < L.ns; ++s) L.w_c[s] = take(W * L.G * 2);
   L.w_cum = take(W);
   L.w_idx = take(W);  // int32 indices stored in double slots
   L.w_misc = take(64);
@@ -236,6 +284,10 @@ inline int make_layout(const afq_dims* d, Layout& L) {
     L.v_acc = take((W * N * 2 * L.nomax + 1) / 2);  // fp32
     for (int s = 0; s < L.ns; ++s) L.v_gt[s] = takeb(W * 2 * L.no[s] * L.Nb, L.v_gt_ps[s]);
   }
+  // scratch whose size follows the tuning record last, so that every buffer
+  // above keeps its offset when the record changes
+  L.w_fbpart = take((long long)L.splitk * 2 * W * L.Gpad);
+  for (int s = 0; s < L.ns; ++s) L.w_exc[s] = take((long long)L.ex[s].mt * W * 2);
   L.work = o;
   return AFQ_OK;
 }

@@ -350,7 +350,7 @@ void base_shape(UmmaParams<Epi>& P, int npc, int M, int N, int K, int batch, int
 }
 
 template <int BN, class Epi>
-int run(UmmaParams<Epi>& P, size_t extra, cudaStream_t st, int prof_id) {
+int run(UmmaParams<Epi>& P, size_t extra, cudaStream_t st, int prof_id, const afq_tuning& T) {
   P.s.stages = umma_pick_stages(BN, P.s.npa, P.s.npb, extra);
   if (P.s.stages < 2 && P.s.kc > 0 && extra == umma_chunk_stage_bytes(BN)) {
     // no room for the chunk staging next to two stages: accumulate in one chunk
@@ -359,8 +359,11 @@ int run(UmmaParams<Epi>& P, size_t extra, cudaStream_t st, int prof_id) {
     P.s.stages = umma_pick_stages(BN, P.s.npa, P.s.npb, extra);
   }
   if (P.s.stages < 2) return AFQ_ERR_SHAPE;
+  if (T.max_stages >= 2 && P.s.stages > T.max_stages) P.s.stages = T.max_stages;
+  int ctas = sm_count();
+  if (T.grid_cap > 0 && T.grid_cap < ctas) ctas = T.grid_cap;
   ProfScope ps(prof_id, st);
-  return launch_umma<BN>(P, extra, sm_count(), st) == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
+  return launch_umma<BN>(P, extra, ctas, st) == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
 }
 
 int* err_flag(const Layout& L, double* work) {
@@ -393,7 +396,7 @@ int prop_launch(const Layout& L, const double* prep, double* work, int s, int nc
   P.epi.wout = wout;
   P.s.ngroups = 2;
   P.s.kc = 4;
-  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_PROP);
+  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
 }
 
 template <int BN>
@@ -422,7 +425,7 @@ int exch_launch(const Layout& L, const double* prep, double* work, int s, cudaSt
   P.epi.wpt = X.wpt;
   P.epi.cout = work + L.w_c[s];
   P.epi.excout = work + L.w_exc[s];
-  return run<BN>(P, ExchEpiU::smem_extra(no), st, K_EXCH);
+  return run<BN>(P, ExchEpiU::smem_extra(no), st, K_EXCH, L.tune);
 }
 
 }  // namespace
@@ -457,8 +460,8 @@ int mixed_prepare(const Layout& L, double* P, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
 }
 
-int mixed_fb_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {
-  constexpr int BN = 128;
+template <int BN>
+int fb_launch(const Layout& L, const double* prep, double* work, cudaStream_t st) {
   UmmaParams<FbEpiU> P{};
   bf16* a[3];
   bf16* b[3];
@@ -485,7 +488,11 @@ int mixed_fb_gemm(const Layout& L, const double* prep, double* work, cudaStream_
   P.epi.zstride = 2LL * L.W * L.Gpad;
   P.s.ngroups = 2;
   P.s.kc = 4;
-  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_FB);
+  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_FB, L.tune);
+}
+
+int mixed_fb_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {
+  return L.fb_bn == 64 ? fb_launch<64>(L, prep, work, st) : fb_launch<128>(L, prep, work, st);
 }
 
 template <int BN>
@@ -508,12 +515,12 @@ int vhs_launch(const Layout& L, const double* prep, double* work, cudaStream_t s
   // K = G accumulates in chunks of 4 K blocks, the hi x hi product apart
   P.s.ngroups = 2;
   P.s.kc = 4;
-  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_VHS);
+  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_VHS, L.tune);
 }
 
 int mixed_vhs_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {
-  // two pieces: 128-wide tiles; three pieces: 64-wide (both keep chunked accumulation)
-  return L.npc == 2 ? vhs_launch<128>(L, prep, work, st) : vhs_launch<64>(L, prep, work, st);
+  // default: two pieces 128-wide tiles, three pieces 64-wide (both keep chunked accumulation)
+  return L.vhs_bn == 128 ? vhs_launch<128>(L, prep, work, st) : vhs_launch<64>(L, prep, work, st);
 }
 
 template <int BN>

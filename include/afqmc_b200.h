@@ -236,6 +236,32 @@ int afq_gemm_split_bf16(const void* const a_pieces[3], int npa, const void* cons
                         int64_t lda, int64_t a_bstride, int64_t ldb, int64_t b_bstride, float* C,
                         int64_t ldc, int64_t c_bstride, int32_t* err_flag, void* stream);
 
+/* Tile and schedule choices of one problem shape (no counterpart in the
+ * reference, where XLA picks its own kernels).  Zero fields keep the built-in
+ * heuristic.  afq_set_tuning registers a record for every call whose afq_dims
+ * equal *d (process-wide, thread-safe); t == NULL removes it.  The workspace
+ * size can depend on the record (split-K partials, exchange partial sums), so
+ * query afq_workspace_size after registering; calls with a smaller workspace
+ * return AFQ_ERR_WORKSPACE.  Buffers that live across calls (Green's
+ * function, per-walker scalars, the error flag) keep their offsets under any
+ * record.  A value the shape cannot use returns AFQ_ERR_ARG and registers
+ * nothing.  afq_get_tuning reports the values in effect (heuristic ones
+ * filled in; max_stages and grid_cap stay 0 when unlimited, and exch_bn is 0
+ * when the exchange runs on the FP64 kernel). */
+typedef struct afq_tuning {
+  int32_t fb_splitk;   /* force-bias GEMM split-K: 1..8                                   */
+  int32_t fb_bn;       /* tensor-core force-bias column tile: 64 or 128                  */
+  int32_t vhs_bn;      /* tensor-core VHS column tile: 64 or 128                          */
+  int32_t exch_bn;     /* tensor-core exchange column tile: 32, 64, 80, 96 or 128         */
+  int32_t f64_exch_bn; /* FP64 exchange tile: 80, 120 or 160 (BM 120, 120, 128)           */
+  int32_t max_stages;  /* cap on tcgen05 pipeline stages: 2..8                             */
+  int32_t grid_cap;    /* CTAs of the persistent tensor-core kernels: 1..number of SMs     */
+  int32_t reserved[9];
+} afq_tuning;
+
+int afq_set_tuning(const afq_dims* d, const afq_tuning* t);
+int afq_get_tuning(const afq_dims* d, afq_tuning* out);
+
 /* Instrumentation (no counterpart in the reference, which has no native
  * code): launches of one kernel family (kernel_id >= 0) or of all library
  * kernels (kernel_id < 0) since load; and CUDA-event timing of every launch
