@@ -29,6 +29,17 @@ struct ExchTile {
   int mt;   // number of row tiles = ceil(G / gpt)
 };
 
+// Shared memory of the tensor-core exchange epilogue: the f block as
+// (re, im) float pairs with an odd row stride in pairs, per-row partials
+// (double4) and per-Cholesky-vector sums (double2) for 128 rows.
+__host__ __device__ inline int exch_fs2(int no) { return (no + 1) | 1; }
+__host__ __device__ inline long long exch_fs_bytes(int no) {
+  return (128LL * exch_fs2(no) * 8 + 31) & ~31LL;
+}
+__host__ __device__ inline long long exch_epi_extra(int no) {
+  return exch_fs_bytes(no) + 128 * 32 + 128 * 16;
+}
+
 // Exchange tile of the tensor-core path: 128 rows hold gpt Cholesky
 // vectors, BN columns hold wpt walkers.
 struct UExchTile {
@@ -42,7 +53,7 @@ inline UExchTile choose_uexch_tile(int no, int G, int npc) {
   UExchTile t;
   const int bns[5] = {128, 96, 80, 64, 32};
   const long long budget = 227 * 1024 - 1024 - 256;
-  const long long extra = ((128LL * (2 * no + 2) * 4 + 31) & ~31LL) + 128 * 32 + 128 * 16;
+  const long long extra = exch_epi_extra(no);
   t.bn = 0;
   double best = -1.0;
   for (int i = 0; i < 5; ++i) {
@@ -65,7 +76,7 @@ inline UExchTile choose_uexch_tile(int no, int G, int npc) {
 inline UExchTile uexch_tile_for(int no, int G, int npc, int bn) {
   UExchTile t{0, 128 / no, 0, 0};
   const long long budget = 227 * 1024 - 1024 - 256;
-  const long long extra = ((128LL * (2 * no + 2) * 4 + 31) & ~31LL) + 128 * 32 + 128 * 16;
+  const long long extra = exch_epi_extra(no);
   const long long stage = (long long)npc * (128 * 128 + bn * 128);
   if (((2 * no + 15) & ~15) <= bn && 2 * stage + extra <= budget) {
     t.bn = bn;

@@ -238,76 +238,143 @@ struct ExchEpiU {
   int G, no, W, gpt, wpt;
   double* cout;    // (W, G) complex
   double* excout;  // (mt, W) complex
+  // Per walker of the tile: stage f (gcount*No rows x 2No floats) in shared
+  // memory as (re, im) pairs, row stride exch_fs2(No) pairs (odd: 64-bit
+  // accesses by consecutive rows or consecutive pairs are bank-conflict free).
+  // Row (g, i) forms sum_j f[i][j] f[j][i] in four FP32 chains combined in
+  // FP64; the rows of one Cholesky vector are summed by a segmented shuffle
+  // reduction inside each warp plus at most three cross-warp partials, then
+  // the Cholesky vectors of the tile by a shuffle reduction in the first
+  // warp.  Every sum has a fixed order, so results are reproducible.
   template <int BN>
   __device__ void tile(int, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t* smem) const {
-    const int nc = 2 * no, fs = nc + 2;  // even stride: float2 reads of (re, im) pairs
-    float* Fs = reinterpret_cast<float*>(smem);
-    double4* pr = reinterpret_cast<double4*>(smem + ((128 * fs * 4 + 31) & ~31));
+    const int nc = 2 * no, fs2 = exch_fs2(no);
+    float2* Fs = reinterpret_cast<float2*>(smem);
+    double4* pr = reinterpret_cast<double4*>(smem + exch_fs_bytes(no));
     double2* ge = reinterpret_cast<double2*>(pr + 128);
     const int g0 = mti * gpt, w0 = nti * wpt;
     const int gcount = min(gpt, G - g0), wcount = min(wpt, W - w0);
     const bool valid = row < gcount * no;
     const int gl = row / no, i = row - (row / no) * no;
+    const int lane = row & 31;
+    const int seg = valid ? gl : -1;
     for (int wl = 0; wl < wcount; ++wl) {
-      const int cb = wl * nc;
+      const int cb = wl * nc;  // even; chunk starts are multiples of 16, so pairs stay aligned
       const int c_lo = cb & ~15, c_hi = (cb + nc + 15) & ~15;
       for (int c = c_lo; c < c_hi; c += 16) {
         float v[16];
         src.load16(c, v);
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
+        for (int k = 0; k < 16; k += 2) {
           const int col = c + k - cb;
-          if (col >= 0 && col < nc) Fs[row * fs + col] = v[k];
+          if (col >= 0 && col < nc) Fs[row * fs2 + (col >> 1)] = make_float2(v[k], v[k + 1]);
         }
       }
       named_sync_epi();
+      double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
       if (valid) {
-        // sum_j f[i][j] f[j][i]: products in FP32, sums in FP64
-        double er = 0.0, ei = 0.0;
-        const float2* fr = reinterpret_cast<const float2*>(Fs + row * fs);
-        const float* fc = Fs + (gl * no) * fs + 2 * i;
-#pragma unroll 4
-        for (int j = 0; j < no; ++j) {
+        const float2* fr = Fs + row * fs2;
+        const float2* fc = Fs + (gl * no) * fs2 + i;
+        float ar[4] = {0.f, 0.f, 0.f, 0.f}, ai[4] = {0.f, 0.f, 0.f, 0.f};
+        int j = 0;
+        for (; j + 4 <= no; j += 4) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float2 a = fr[j + u];
+            const float2 b = fc[(j + u) * fs2];
+            ar[u] = fmaf(a.x, b.x, fmaf(-a.y, b.y, ar[u]));
+            ai[u] = fmaf(a.x, b.y, fmaf(a.y, b.x, ai[u]));
+          }
+        }
+        for (; j < no; ++j) {
           const float2 a = fr[j];
-          const float2 b = *reinterpret_cast<const float2*>(fc + j * fs);
-          er += (double)(a.x * b.x) - (double)(a.y * b.y);
-          ei += (double)(a.x * b.y) + (double)(a.y * b.x);
+          const float2 b = fc[j * fs2];
+          ar[0] = fmaf(a.x, b.x, fmaf(-a.y, b.y, ar[0]));
+          ai[0] = fmaf(a.x, b.y, fmaf(a.y, b.x, ai[0]));
         }
         const float2 d = fr[i];
-        pr[row] = make_double4(er, ei, (double)d.x, (double)d.y);
+        q = make_double4(((double)ar[0] + (double)ar[1]) + ((double)ar[2] + (double)ar[3]),
+                         ((double)ai[0] + (double)ai[1]) + ((double)ai[2] + (double)ai[3]),
+                         (double)d.x, (double)d.y);
       }
-      named_sync_epi();
-      if (row < gcount) {
-        double sr = 0, si = 0, tr = 0, ti = 0;
-        for (int ii = 0; ii < no; ++ii) {
-          const double4 q = pr[row * no + ii];
-          sr += q.x;
-          si += q.y;
-          tr += q.z;
-          ti += q.w;
+      // suffix sums inside each run of equal `seg` within the warp
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double tx = __shfl_down_sync(0xffffffffu, q.x, off);
+        const double ty = __shfl_down_sync(0xffffffffu, q.y, off);
+        const double tz = __shfl_down_sync(0xffffffffu, q.z, off);
+        const double tw = __shfl_down_sync(0xffffffffu, q.w, off);
+        const int st = __shfl_down_sync(0xffffffffu, seg, off);
+        if (lane + off < 32 && st == seg) {
+          q.x += tx;
+          q.y += ty;
+          q.z += tz;
+          q.w += tw;
         }
-        const long long co = 2 * ((long long)(w0 + wl) * G + g0 + row);
-        cout[co] = tr;
-        cout[co + 1] = ti;
-        ge[row] = make_double2(sr, si);
       }
+      const int sp = __shfl_up_sync(0xffffffffu, seg, 1);
+      if (valid && (lane == 0 || sp != seg)) pr[row] = q;  // run heads
       named_sync_epi();
-      if (row == 0) {
-        double sx = 0, sy = 0;
-        for (int g = 0; g < gcount; ++g) {
-          sx += ge[g].x;
-          sy += ge[g].y;
+      if (gcount <= 32) {
+        if (row < 32) {
+          double sr = 0.0, si = 0.0;
+          if (row < gcount) {
+            const int h = row * no;
+            double4 a = pr[h];
+            for (int r = (h / 32 + 1) * 32; r < h + no; r += 32) {
+              const double4 b = pr[r];
+              a.x += b.x;
+              a.y += b.y;
+              a.z += b.z;
+              a.w += b.w;
+            }
+            const long long co = 2 * ((long long)(w0 + wl) * G + g0 + row);
+            cout[co] = a.z;
+            cout[co + 1] = a.w;
+            sr = a.x;
+            si = a.y;
+          }
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            sr += __shfl_down_sync(0xffffffffu, sr, off);
+            si += __shfl_down_sync(0xffffffffu, si, off);
+          }
+          if (row == 0) {
+            excout[2 * ((long long)mti * W + w0 + wl)] = sr;
+            excout[2 * ((long long)mti * W + w0 + wl) + 1] = si;
+          }
         }
-        excout[2 * ((long long)mti * W + w0 + wl)] = sx;
-        excout[2 * ((long long)mti * W + w0 + wl) + 1] = sy;
+      } else {  // more than 32 Cholesky vectors per tile (No < 4)
+        if (row < gcount) {
+          const int h = row * no;
+          double4 a = pr[h];
+          for (int r = (h / 32 + 1) * 32; r < h + no; r += 32) {
+            const double4 b = pr[r];
+            a.x += b.x;
+            a.y += b.y;
+            a.z += b.z;
+            a.w += b.w;
+          }
+          const long long co = 2 * ((long long)(w0 + wl) * G + g0 + row);
+          cout[co] = a.z;
+          cout[co + 1] = a.w;
+          ge[row] = make_double2(a.x, a.y);
+        }
+        named_sync_epi();
+        if (row == 0) {
+          double sx = 0, sy = 0;
+          for (int g = 0; g < gcount; ++g) {
+            sx += ge[g].x;
+            sy += ge[g].y;
+          }
+          excout[2 * ((long long)mti * W + w0 + wl)] = sx;
+          excout[2 * ((long long)mti * W + w0 + wl) + 1] = sy;
+        }
       }
     }
   }
-  static size_t smem_extra(int no) {
-    const int fs = 2 * no + 2;
-    return ((size_t(128) * fs * 4 + 31) & ~size_t(31)) + 128 * sizeof(double4) + 128 * sizeof(double2);
-  }
+  static size_t smem_extra(int no) { return exch_epi_extra(no); }
 };
 
 // ---------------------------------------------------------------------------
