@@ -37,16 +37,24 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
   const int ts = no + 1;  // padded row stride of tstage (conflict-free column reads)
   __shared__ double red[2 * (T / 32)];
   __shared__ int perm[64];
-  __shared__ int piv_s;
 
   const double2* Wg =
       reinterpret_cast<const double2*>(S_.walk) + (long long)w * N * no;
 
-  // ---- S = C^T W -----------------------------------------------------------
-  const int npairs = no * no;
-  double2 acc[16];
+  // ---- S = C^T W on the FP64 tensor cores ----------------------------------
+  // As real matrices: S (No x 2No, (re, im) interleaved) = C^T (No x N) times
+  // W (N x 2No, the complex walker viewed as doubles).  mma.m8n8k4 tiles: warp
+  // w owns column tiles w and w + 8 and every row tile, so each B fragment is
+  // loaded once per k-step.  Rows of W and C are staged 32 at a time.
+  const int warp = tid >> 5, lane = tid & 31;
+  const int nc2 = 2 * no;
+  const int mtiles = (no + 7) >> 3, ntiles = (nc2 + 7) >> 3;  // <= 8, <= 16
+  const double* stageD = reinterpret_cast<const double*>(stage);
+  double sacc[2][8][2];
 #pragma unroll
-  for (int q = 0; q < 16; ++q) acc[q] = make_double2(0.0, 0.0);
+  for (int sl = 0; sl < 2; ++sl)
+#pragma unroll
+    for (int mi = 0; mi < 8; ++mi) sacc[sl][mi][0] = sacc[sl][mi][1] = 0.0;
   for (int p0 = 0; p0 < N; p0 += kRowChunk) {
     const int rows = min(kRowChunk, N - p0);
     for (int e = tid; e < rows * no; e += T) {
@@ -54,37 +62,63 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
       moc[e] = S_.mo[(long long)p0 * no + e];
     }
     __syncthreads();
+    for (int kk = 0; kk < rows; kk += 4) {
+      const int kr = kk + (lane & 3);
+      const bool kin = kr < rows;
+      double afr[8];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int pr = tid + q * T;
-      if (pr < npairs) {
-        const int i = pr / no, j = pr - (pr / no) * no;
-        double2 s = acc[q];
-        for (int r = 0; r < rows; ++r) {
-          const double c = moc[r * no + i];
-          const double2 x = stage[r * no + j];
-          s.x = fma(c, x.x, s.x);
-          s.y = fma(c, x.y, s.y);
+      for (int mi = 0; mi < 8; ++mi) {
+        const int m = mi * 8 + (lane >> 2);
+        afr[mi] = (mi < mtiles && kin && m < no) ? moc[kr * no + m] : 0.0;
+      }
+#pragma unroll
+      for (int sl = 0; sl < 2; ++sl) {
+        const int ni = warp + sl * 8;
+        if (ni < ntiles) {  // warp-uniform
+          const int n = ni * 8 + (lane >> 2);
+          const double b = (kin && n < nc2) ? stageD[kr * nc2 + n] : 0.0;
+#pragma unroll
+          for (int mi = 0; mi < 8; ++mi)
+            if (mi < mtiles) dmma_8x8x4(sacc[sl][mi][0], sacc[sl][mi][1], afr[mi], b);
         }
-        acc[q] = s;
       }
     }
     __syncthreads();
   }
+  const int npairs = no * no;
 #pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    const int pr = tid + q * T;
-    if (pr < npairs) S[pr] = acc[q];
+  for (int sl = 0; sl < 2; ++sl) {
+    const int ni = warp + sl * 8;
+    if (ni < ntiles) {
+#pragma unroll
+      for (int mi = 0; mi < 8; ++mi) {
+        const int i = mi * 8 + (lane >> 2), j = ni * 4 + (lane & 3);
+        if (mi < mtiles && i < no && j < no)
+          S[i * no + j] = make_double2(sacc[sl][mi][0], sacc[sl][mi][1]);
+      }
+    }
   }
   __syncthreads();
 
   // ---- Gauss-Jordan inverse with partial pivoting, det ----------------------
+  // Each elimination step: warp 0 alone finds the pivot (first max of
+  // |re|+|im| in column k, as LAPACK izamax), swaps it into row k, keeps
+  // column k and scales row k by 1/p (= conj(p)/|p|^2); then every thread
+  // updates its fixed elements.  Two block barriers per step.
+  __shared__ double2 ipk_s;
+  int my_i[16], my_j[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int e = tid + q * T;
+    my_i[q] = e < npairs ? e / no : -1;
+    my_j[q] = e < npairs ? e - (e / no) * no : 0;
+  }
   double2 det = make_double2(1.0, 0.0);
   for (int k = 0; k < no; ++k) {
-    if (tid < 32) {
+    if (warp == 0) {
       double best = -1.0;
       int bi = k;
-      for (int r = k + tid; r < no; r += 32) {
+      for (int r = k + lane; r < no; r += 32) {
         const double2 v = S[r * no + k];
         const double m = fabs(v.x) + fabs(v.y);
         if (m > best) { best = m; bi = r; }
@@ -95,52 +129,54 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
         const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
         if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
       }
-      if (tid == 0) { piv_s = bi; perm[k] = bi; }
-    }
-    __syncthreads();
-    const int pv = piv_s;
-    if (pv != k) {
-      for (int j = tid; j < no; j += T) {
-        const double2 t0 = S[k * no + j];
-        S[k * no + j] = S[pv * no + j];
-        S[pv * no + j] = t0;
+      const int pv = bi;
+      if (pv != k)
+        for (int j = lane; j < no; j += 32) {
+          const double2 t0 = S[k * no + j];
+          S[k * no + j] = S[pv * no + j];
+          S[pv * no + j] = t0;
+        }
+      __syncwarp();
+      const double2 pk = S[k * no + k];
+      const double inv = 1.0 / (pk.x * pk.x + pk.y * pk.y);
+      const double2 ipk = make_double2(pk.x * inv, -pk.y * inv);
+      for (int i = lane; i < no; i += 32) colk[i] = S[i * no + k];
+      __syncwarp();
+      for (int j = lane; j < no; j += 32) S[k * no + j] = (j == k) ? ipk : cmul(S[k * no + j], ipk);
+      if (lane == 0) {
+        perm[k] = pv;
+        ipk_s = ipk;
+        det = cmul(det, pk);
+        if (pv != k) det = make_double2(-det.x, -det.y);
       }
     }
     __syncthreads();
-    const double2 pk = S[k * no + k];
-    const double2 ipk = cdiv(make_double2(1.0, 0.0), pk);
-    for (int i = tid; i < no; i += T) colk[i] = S[i * no + k];
-    if (tid == 0) {
-      det = cmul(det, pk);
-      if (pv != k) det = make_double2(-det.x, -det.y);
-    }
-    __syncthreads();
-    for (int j = tid; j < no; j += T) S[k * no + j] = (j == k) ? ipk : cmul(S[k * no + j], ipk);
-    __syncthreads();
-    for (int e = tid; e < npairs; e += T) {
-      const int i = e / no, j = e - (e / no) * no;
-      if (i == k) continue;
+    const double2 ipk = ipk_s;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int i = my_i[q], j = my_j[q];
+      if (i < 0 || i == k) continue;
       const double2 f = colk[i];
       if (j == k) {
         const double2 t0 = cmul(f, ipk);
-        S[e] = make_double2(-t0.x, -t0.y);
+        S[i * no + j] = make_double2(-t0.x, -t0.y);
       } else {
-        S[e] = csub(S[e], cmul(f, S[k * no + j]));
+        S[i * no + j] = csub(S[i * no + j], cmul(f, S[k * no + j]));
       }
     }
     __syncthreads();
   }
-  for (int k = no - 1; k >= 0; --k) {
-    const int pv = perm[k];
-    if (pv != k) {
-      for (int i = tid; i < no; i += T) {
+  // undo the row interchanges as column interchanges, last first (rows independent)
+  for (int i = tid; i < no; i += T)
+    for (int k = no - 1; k >= 0; --k) {
+      const int pv = perm[k];
+      if (pv != k) {
         const double2 t0 = S[i * no + k];
         S[i * no + k] = S[i * no + pv];
         S[i * no + pv] = t0;
       }
     }
-    __syncthreads();
-  }
+  __syncthreads();
   if (tid == 0 && a.wscal) {
     a.wscal[(long long)w * 16 + 4 + 2 * sct] = det.x;
     a.wscal[(long long)w * 16 + 5 + 2 * sct] = det.y;
@@ -162,22 +198,59 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
     // walker rows of this chunk into shared memory
     for (int e = tid; e < rows * no; e += T) stage[e] = Wg[(long long)p0 * no + e];
     __syncthreads();
-    for (int e = tid; e < rows * no; e += T) {
-      const int r = e / no, j = e - (e / no) * no;
-      const double2* wrow = stage + r * no;
-      double2 s = make_double2(0.0, 0.0);
-      for (int i = 0; i < no; ++i) {
-        const double2 x = wrow[i];
-        const double2 y = S[i * no + j];
-        s.x = fma(x.x, y.x, fma(-x.y, y.y, s.x));
-        s.y = fma(x.x, y.y, fma(x.y, y.x, s.y));
+    // Theta rows (N x 2No real) = W rows (N x 2No) times the real form of
+    // S^-1: R[2i][2j] = R[2i+1][2j+1] = Re s_ij, R[2i][2j+1] = Im s_ij,
+    // R[2i+1][2j] = -Im s_ij, generated in the B fragments
+    {
+      const int rtiles = (rows + 7) >> 3;  // <= 4
+      double tacc[2][4][2];
+#pragma unroll
+      for (int sl = 0; sl < 2; ++sl)
+#pragma unroll
+        for (int ri = 0; ri < 4; ++ri) tacc[sl][ri][0] = tacc[sl][ri][1] = 0.0;
+      for (int kk = 0; kk < nc2; kk += 4) {
+        const int k = kk + (lane & 3);
+        const bool kin = k < nc2;
+        double afr[4];
+#pragma unroll
+        for (int ri = 0; ri < 4; ++ri) {
+          const int r = ri * 8 + (lane >> 2);
+          afr[ri] = (ri < rtiles && kin && r < rows) ? stageD[r * nc2 + k] : 0.0;
+        }
+#pragma unroll
+        for (int sl = 0; sl < 2; ++sl) {
+          const int ni = warp + sl * 8;
+          if (ni < ntiles) {  // warp-uniform
+            const int n = ni * 8 + (lane >> 2);
+            double b = 0.0;
+            if (kin && n < nc2) {
+              const double2 sv = S[(k >> 1) * no + (n >> 1)];
+              b = (k & 1) == 0 ? ((n & 1) == 0 ? sv.x : sv.y) : ((n & 1) == 0 ? -sv.y : sv.x);
+            }
+#pragma unroll
+            for (int ri = 0; ri < 4; ++ri)
+              if (ri < rtiles) dmma_8x8x4(tacc[sl][ri][0], tacc[sl][ri][1], afr[ri], b);
+          }
+        }
       }
-      tstage[r * ts + j] = s;
-      if (th) th[(long long)(p0 + r) * no + j] = s;
-      if (S_.rh1) {
-        const double h = S_.rh1[(long long)j * N + p0 + r];
-        e1.x = fma(s.x, h, e1.x);
-        e1.y = fma(s.y, h, e1.y);
+#pragma unroll
+      for (int sl = 0; sl < 2; ++sl) {
+        const int ni = warp + sl * 8;
+        if (ni >= ntiles) continue;
+#pragma unroll
+        for (int ri = 0; ri < 4; ++ri) {
+          const int r = ri * 8 + (lane >> 2), j = ni * 4 + (lane & 3);
+          if (ri < rtiles && r < rows && j < no) {
+            const double2 sv = make_double2(tacc[sl][ri][0], tacc[sl][ri][1]);
+            tstage[r * ts + j] = sv;
+            if (th) th[(long long)(p0 + r) * no + j] = sv;
+            if (S_.rh1) {
+              const double h = S_.rh1[(long long)j * N + p0 + r];
+              e1.x = fma(sv.x, h, e1.x);
+              e1.y = fma(sv.y, h, e1.y);
+            }
+          }
+        }
       }
     }
     __syncthreads();
