@@ -371,7 +371,7 @@ static int sr_impl(const afq_dims* d, const double* weights_in, double zeta, con
   if (L.W > kMaxSrWalkers) return AFQ_ERR_SHAPE;
   if (weights_out == weights_in) return AFQ_ERR_ARG;
   cudaStream_t st = as_stream(stream);
-  AFQ_TRY(launch_sr(L.W, weights_in, zeta, zeta_dev, mode, weights_out, indices, st));
+  AFQ_TRY(launch_sr(L.W, 1, weights_in, zeta, zeta_dev, mode, weights_out, indices, st));
   if (walkers_in && walkers_out) {
     for (int s = 0; s < L.ns; ++s) {
       if (!walkers_in[s] || !walkers_out[s]) return AFQ_ERR_NULL;
@@ -399,6 +399,18 @@ int afq_stochastic_reconfiguration_dev(const afq_dims* d, const double* weights_
   if (!zeta_dev) return AFQ_ERR_NULL;
   return sr_impl(d, weights_in, 0.0, zeta_dev, mode, walkers_in, walkers_out, weights_out,
                  indices, stream);
+}
+
+int afq_comb_indices_ranks(const double* weights_all, int32_t n_per_rank, int32_t n_ranks,
+                           double zeta, double* weights_out, int32_t* indices, void* stream) {
+  if (!weights_all || !weights_out || !indices) return AFQ_ERR_NULL;
+  if (n_per_rank <= 0 || n_ranks <= 0) return AFQ_ERR_SHAPE;
+  const long long W = (long long)n_per_rank * n_ranks;
+  if (W > kMaxSrWalkers) return AFQ_ERR_SHAPE;
+  if (weights_out == weights_all) return AFQ_ERR_ARG;
+  AFQ_TRY(launch_sr((int)W, n_ranks, weights_all, zeta, nullptr, AFQ_SR_GLOBAL, weights_out,
+                    indices, as_stream(stream)));
+  return AFQ_OK;
 }
 
 int afq_block_end(const afq_dims* d, const void* prepared, afq_state* s, double* block_out,

@@ -58,8 +58,9 @@ cudaError_t launch_qr(const Layout& L, double* const walkers[2], double* norms, 
                       cudaStream_t st);
 // W <= kMaxSrWalkers (cumulative sum kept in shared memory)
 constexpr int kMaxSrWalkers = 16384;
-cudaError_t launch_sr(int W, const double* weights_in, double zeta, const double* zeta_dev,
-                      int mode, double* weights_out, int* indices, cudaStream_t st);
+cudaError_t launch_sr(int W, int ranks, const double* weights_in, double zeta,
+                      const double* zeta_dev, int mode, double* weights_out, int* indices,
+                      cudaStream_t st);
 cudaError_t launch_gather(int W, long long walker_doubles, const double* in, double* out,
                           const int* indices, cudaStream_t st);
 cudaError_t launch_block_end(const Layout& L, double* work, const double* weights,

@@ -227,8 +227,10 @@ __global__ void qr_norm_kernel(int W, int ns, int restricted, const double* sect
 // comb reconfiguration (single CTA); bit-exact: serial cumsum, explicit
 // round-to-nearest arithmetic in the reference's expression order.
 // ---------------------------------------------------------------------------
-__global__ void sr_kernel(int W, const double* win, double zeta_host, const double* zeta_dev,
-                          int mode, double* wout, int* idx) {
+// W slots over `ranks` ranks of W / ranks walkers each (ranks = 1 except for
+// the reconfiguration across ranks, which combs the gathered weights)
+__global__ void sr_kernel(int W, int ranks, const double* win, double zeta_host,
+                          const double* zeta_dev, int mode, double* wout, int* idx) {
   extern __shared__ double cum[];
   const double zeta = zeta_dev ? *zeta_dev : zeta_host;
   if (threadIdx.x == 0) {
@@ -241,12 +243,13 @@ __global__ void sr_kernel(int W, const double* win, double zeta_host, const doub
   __syncthreads();
   const double total = cum[W - 1];
   const double dW = (double)W;
+  const double dWr = (double)(W / ranks), dR = (double)ranks;  // per-rank count, ranks
   for (int i = threadIdx.x; i < W; i += blockDim.x) {
     double z;
     if (mode == AFQ_SR_LOCAL)
       z = __ddiv_rn(__dmul_rn(total, __dadd_rn((double)i, zeta)), dW);
-    else
-      z = __dmul_rn(__ddiv_rn(__ddiv_rn(__dadd_rn((double)i, zeta), dW), 1.0), total);
+    else  // (i + zeta) / nwalkers / size * total, nwalkers per rank
+      z = __dmul_rn(__ddiv_rn(__ddiv_rn(__dadd_rn((double)i, zeta), dWr), dR), total);
     int lo = 0, hi = W;
     while (lo < hi) {
       const int mid = (lo + hi) >> 1;
@@ -256,7 +259,7 @@ __global__ void sr_kernel(int W, const double* win, double zeta_host, const doub
         hi = mid;
     }
     idx[i] = lo < W ? lo : W - 1;
-    wout[i] = (mode == AFQ_SR_LOCAL) ? __ddiv_rn(total, dW) : __ddiv_rn(__ddiv_rn(total, dW), 1.0);
+    wout[i] = (mode == AFQ_SR_LOCAL) ? __ddiv_rn(total, dW) : __ddiv_rn(__ddiv_rn(total, dWr), dR);
   }
 }
 
@@ -415,14 +418,16 @@ cudaError_t launch_qr(const Layout& L, double* const walkers[2], double* norms, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_sr(int W, const double* weights_in, double zeta, const double* zeta_dev,
-                      int mode, double* weights_out, int* indices, cudaStream_t st) {
+cudaError_t launch_sr(int W, int ranks, const double* weights_in, double zeta,
+                      const double* zeta_dev, int mode, double* weights_out, int* indices,
+                      cudaStream_t st) {
   const size_t smem = size_t(W) * sizeof(double);
   cudaError_t e =
       cudaFuncSetAttribute(sr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   ProfScope ps(K_SR, st);
-  sr_kernel<<<1, 1024, smem, st>>>(W, weights_in, zeta, zeta_dev, mode, weights_out, indices);
+  sr_kernel<<<1, 1024, smem, st>>>(W, ranks, weights_in, zeta, zeta_dev, mode, weights_out,
+                                   indices);
   return cudaGetLastError();
 }
 

@@ -35,13 +35,19 @@ from .walkers import UHFWalkers
 
 class BlockGraph:
     def __init__(self, ham, ham_data, prop, trial, wave_data, prop_data, n_prop_steps: int = 10,
-                 update_estimate: bool = True):
+                 update_estimate: bool = True, reconfigure: bool = True):
+        """reconfigure=False leaves the comb (and the overlaps of the new
+        walkers) out of the recorded block, for callers that reconfigure
+        across ranks after each replay; update_estimate=False leaves out the
+        e_estimate update (a caller with several ranks updates it from the
+        all-reduced block energy)."""
         self.prop, self.trial, self.wave_data, self.ham_data = prop, trial, wave_data, ham_data
         self.eng = prop.engine(ham_data, trial, wave_data)
         if not self.eng.has_prop:
             raise _lib.AfqError("propagation intermediates missing")
         self.S = int(n_prop_steps)
         self.update_estimate = update_estimate
+        self.reconfigure = reconfigure
         self.pd = prop_data
         sync_scalars(prop_data)
         w = prop_data["walkers"]
@@ -82,6 +88,13 @@ class BlockGraph:
                        "afq_propagate_constrained")
         _lib.check(lib.afq_block_end(C.byref(eng.dims), p, C.byref(st), self.block_out.data_ptr(), w,
                                      wb, stream), "afq_block_end")
+        if not self.reconfigure:
+            sc[2].div_(self.prop.n_walkers)
+            if self.update_estimate:
+                sc[0].mul_(0.9).add_(0.1 * self.block_out[0])
+            self.launches_per_block = _lib.launch_count() - n0
+            pd.pop("_afq_green_of", None)
+            return
         _lib.check(lib.afq_uniform_dev(self.zeta.data_ptr(), self.seed, self.counter.data_ptr(), stream),
                    "afq_uniform_dev")
         win = _lib.pair(*[t.data_ptr() for t in self.tensors] + [None] * (2 - len(self.tensors)))

@@ -31,6 +31,22 @@ def _as_weights(weights) -> torch.Tensor:
     return to_dev(weights, torch.float64)
 
 
+def _multi_rank(comm) -> bool:
+    """True for a torch.distributed group of more than one rank.  An MPI-style
+    communicator (Get_size) of one rank keeps the single-rank path; the
+    reconfiguration across ranks runs on torch.distributed groups."""
+    if comm is None:
+        return False
+    if hasattr(comm, "Get_size"):
+        if comm.Get_size() == 1:
+            return False
+        raise ValueError("reconfiguration across ranks takes a torch.distributed process group "
+                         "(one rank per GPU), not an MPI communicator")
+    import torch.distributed as dist
+
+    return dist.is_initialized() and dist.get_world_size(comm) > 1
+
+
 class walker_batch:
     """Common interface (walkers.py:11-82)."""
 
@@ -91,7 +107,14 @@ class RHFWalkers(walker_batch):
         return self.__class__(outs[0]), w
 
     def stochastic_reconfiguration_global(self, weights, zeta, comm=None):
-        """walkers.py:147-153 -> sr.py:52-92 on a single rank."""
+        """walkers.py:147-153 -> sr.py:52-92.  ``comm``: a torch.distributed
+        process group (one rank per GPU; the same zeta on every rank) for the
+        reconfiguration across ranks (sr_ranks.py), None for one rank."""
+        if _multi_rank(comm):
+            from .sr_ranks import reconfigure_across_ranks
+
+            outs, w = reconfigure_across_ranks([self.data], to_dev(weights), float(zeta), comm)
+            return self.__class__(outs[0]), w
         outs, w, _ = self._sr([self.data], weights, zeta, _lib.AFQ_SR_GLOBAL, "restricted")
         return self.__class__(outs[0]), w
 
@@ -130,7 +153,12 @@ class UHFWalkers(walker_batch):
         return self.__class__(outs), w
 
     def stochastic_reconfiguration_global(self, weights, zeta, comm=None):
-        """walkers.py:252-258 -> sr.py:95-153 on a single rank."""
+        """walkers.py:252-258 -> sr.py:95-153; ``comm`` as for RHFWalkers."""
+        if _multi_rank(comm):
+            from .sr_ranks import reconfigure_across_ranks
+
+            outs, w = reconfigure_across_ranks(list(self.data), to_dev(weights), float(zeta), comm)
+            return self.__class__(outs), w
         outs, w, _ = self._sr(self.data, weights, zeta, _lib.AFQ_SR_GLOBAL, "unrestricted")
         return self.__class__(outs), w
 

@@ -214,15 +214,31 @@ def main():
     def timed_run(precision, steps, warmup, profile_kernel=None, graph=False):
         hd, wv, pr, pd_ = setup(sys_, precision, 1000 + rank)
         if graph:
-            # the block (fields, 10 steps, block end, comb, e_estimate update) as one CUDA graph
+            # the block (fields, 10 steps, block end, comb, e_estimate update) as one CUDA graph;
+            # with several ranks the comb and the estimate update follow the reference driver
+            # (driver.py:133-168): block energy all-reduced (weighted), walkers reconfigured
+            # across ranks (sr_ranks.py), e_estimate from the global block energy
             from ad_afqmc_b200.graphs import BlockGraph
-            bg = BlockGraph(ham, hd, pr, trial, wv, pd_, n_prop_steps=S).capture(warmup=1)
+            multi = world > 1
+            bg = BlockGraph(ham, hd, pr, trial, wv, pd_, n_prop_steps=S, reconfigure=not multi,
+                            update_estimate=not multi).capture(warmup=1)
+            zeta_rng = np.random.default_rng(97)  # identical stream on every rank
 
             def run_block():
-                e = bg.replay()[0]
-                if world > 1:
-                    t = torch.stack([e * torch.sum(pd_["weights"]), torch.sum(pd_["weights"])])
+                out = bg.replay()
+                if multi:
+                    wsum = torch.sum(pd_["weights"])
+                    t = torch.stack([out[0] * wsum, wsum])
                     dist.all_reduce(t)
+                    e_glob = t[0] / t[1]
+                    new, w_new = pd_["walkers"].stochastic_reconfiguration_global(
+                        pd_["weights"], float(zeta_rng.random()), dist.group.WORLD)
+                    for dst, src in zip(bg.tensors, new.data if isinstance(new.data, list) else [new.data]):
+                        dst.copy_(src)
+                    pd_["weights"].copy_(w_new)
+                    pd_["overlaps"].copy_(trial.calc_overlap(pd_["walkers"], wv))
+                    sc = pd_["_scalars"]
+                    sc[0].mul_(0.9).add_(0.1 * e_glob)
         else:
             smp_ = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1)
 
@@ -250,7 +266,7 @@ def main():
         kern = _lib.profile_end() if (profile_kernel and not graph) else (0.0, 0)
         launches = _lib.launch_count() - n0
         if graph:
-            launches = bg.launches_per_block * steps
+            launches = bg.launches_per_block * steps + launches  # + eager launches (several ranks)
             if profile_kernel:
                 # the dominant kernel timed with CUDA events in eager blocks of the same state
                 smp_ = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1)
@@ -393,7 +409,9 @@ def main():
            "data": "synthetic",
            "config": {"workload": args.config, "norb": N, "nelec": list(sys_.nelec), "nchol": G,
                       "n_walkers_per_gpu": W, "n_prop_steps_per_bench_step": S, "dt": dt,
-                      "precision": args.precision, "parallelism": f"replicas x{world}",
+                      "precision": args.precision,
+                      "parallelism": (f"dp{world}: walkers sharded by rank, block energy all-reduced, "
+                                      "reconfiguration across ranks every block") if world > 1 else "1 GPU",
                       "l2": "working set (VHS 328 MB, chol 320 MB) exceeds the 126 MB L2",
                       "chol_scale": args.chol_scale, "killed_walker_fraction": killed,
                       "launch": "eager" if args.eager else "cuda_graph_per_block"},

@@ -188,6 +188,18 @@ int afq_stochastic_reconfiguration(const afq_dims* d, const double* weights_in, 
                                    double* const walkers_out[2], double* weights_out,
                                    int32_t* indices, void* stream);
 
+/* Comb of the reconfiguration across ranks: weights_all holds the weights
+ * of n_ranks ranks of n_per_rank walkers each, in rank order (an all-gather).
+ * Writes, for every one of the n_ranks * n_per_rank slots, the global index of
+ * the walker that fills it and its new weight, with the rank-0 arithmetic of
+ * sr.py:52-153 (z = (i + zeta) / n_per_rank / n_ranks * total, serial FP64
+ * cumsum, searchsorted left): bit-exact given identical weights and zeta, so
+ * every rank can comb the same gathered weights and agree on the plan.  The
+ * walkers then move with one all-to-all (ad_afqmc_b200/sr_ranks.py).
+ * n_ranks * n_per_rank <= 16384.  Device pointers. */
+int afq_comb_indices_ranks(const double* weights_all, int32_t n_per_rank, int32_t n_ranks,
+                           double zeta, double* weights_out, int32_t* indices, void* stream);
+
 /* As afq_stochastic_reconfiguration with zeta read from device memory, so
  * that the call can be recorded in a CUDA graph and replayed with fresh
  * uniforms (see afq_uniform_dev). */
