@@ -401,6 +401,25 @@ int afq_stochastic_reconfiguration_dev(const afq_dims* d, const double* weights_
                  indices, stream);
 }
 
+int afq_calc_orbenergy(const afq_dims* d, const void* prepared, const double* const walkers[2],
+                       const double* prjlo, int32_t n_lo, double* orbe, void* work,
+                       size_t work_bytes, void* stream) {
+  Layout L;
+  int rc = check_common(d, L, prepared, work, work_bytes);
+  if (rc != AFQ_OK) return rc;
+  if (!walkers || !walkers[0] || !prjlo || !orbe) return AFQ_ERR_NULL;
+  if (!L.restricted || L.uhf_trial) return AFQ_ERR_ARG;  // rhf_lno with restricted walkers
+  if (n_lo < 1 || n_lo > 8) return AFQ_ERR_ARG;
+  const double* prep = static_cast<const double*>(prepared);
+  double* wk = static_cast<double*>(work);
+  cudaStream_t st = as_stream(stream);
+  GreenArgs a = green_args(L, prep, wk, walkers);
+  a.sec[0].theta = wk + L.w_theta[0];
+  AFQ_TRY(launch_green(a, st));
+  AFQ_TRY(launch_orbenergy(L, prep, wk, prjlo, n_lo, orbe, st));
+  return AFQ_OK;
+}
+
 int afq_comb_indices_ranks(const double* weights_all, int32_t n_per_rank, int32_t n_ranks,
                            double zeta, double* weights_out, int32_t* indices, void* stream) {
   if (!weights_all || !weights_out || !indices) return AFQ_ERR_NULL;

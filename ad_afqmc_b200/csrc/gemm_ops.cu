@@ -261,6 +261,115 @@ __global__ void __launch_bounds__(Cfg::NT) exch_kernel(F64Operand A, F64Operand 
 }
 
 // ---------------------------------------------------------------------------
+// LNO orbital energy (rhf_lno._calc_orbenergy, wavefunctions.py:6904-6923):
+// f = RC[g] . Theta_vir per (Cholesky vector, walker), Theta's occupied rows
+// zeroed beforehand (so only rot_chol's virtual columns contribute), staged
+// in shared memory as in the exchange.  With m = sum_r p_r^T p_r (prjlo rows
+// p_r): c = tr f, s1 = sum_r p_r f p_r^T (= sum f o m), s2 = sum_r (p_r f).(f
+// p_r^T) (= sum (f f) o m); the tile's partial sum_g (2 c s1 - s2) per walker.
+// ---------------------------------------------------------------------------
+constexpr int kMaxLo = 8;
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT) orb_kernel(F64Operand A, F64Operand B, int G, int no,
+                                                      int N, int W, int gpt, int wpt,
+                                                      const double* prj, int nlo, double* orbout) {
+  extern __shared__ double smem[];
+  const int mt = blockIdx.x, nt = blockIdx.y;
+  const int g0 = mt * gpt, w0 = nt * wpt;
+  const int gcount = min(gpt, G - g0), wcount = min(wpt, W - w0);
+  const int m0 = g0 * no, n0 = w0 * 2 * no;
+  const int M_lim = (g0 + gcount) * no, N_lim = (w0 + wcount) * 2 * no;
+  double acc[Cfg::FM][Cfg::FN][2];
+  f64_zero<Cfg>(acc);
+  f64_mainloop<Cfg, B_KMAJOR>(acc, A, B, M_lim, N_lim, 0, N, m0, n0, 0, false, smem);
+
+  constexpr int CS = Cfg::BN + 2;
+  double* Ct = smem;
+  double* P = smem + Cfg::BM * CS;  // nlo x no projector rows
+  double2* blk = reinterpret_cast<double2*>(P + kMaxLo * 64);
+  f64_foreach<Cfg>(acc, 0, 0, [&](int m, int n, double v0, double v1) {
+    *reinterpret_cast<double2*>(Ct + m * CS + n) = make_double2(v0, v1);
+  });
+  for (int e = threadIdx.x; e < nlo * no; e += Cfg::NT) P[e] = prj[e];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = Cfg::NT / 32;
+  const int nblk = gcount * wcount;
+  for (int bi = warp; bi < nblk; bi += nwarps) {
+    const int gl = bi % gcount, wl = bi / gcount;
+    const double* F = Ct + gl * no * CS + wl * 2 * no;
+    double cr = 0, ci = 0, ar = 0, ai = 0, br = 0, bi_ = 0;
+    for (int k = lane; k < no; k += 32) {
+      cr += F[k * CS + 2 * k];
+      ci += F[k * CS + 2 * k + 1];
+    }
+    for (int r = 0; r < nlo; ++r) {
+      const double* p = P + r * no;
+      for (int k = lane; k < no; k += 32) {
+        double ur = 0, ui = 0, vr = 0, vi = 0;  // u = (p f)[k], v = (f p^T)[k]
+        for (int x = 0; x < no; ++x) {
+          ur = fma(p[x], F[x * CS + 2 * k], ur);
+          ui = fma(p[x], F[x * CS + 2 * k + 1], ui);
+          vr = fma(F[k * CS + 2 * x], p[x], vr);
+          vi = fma(F[k * CS + 2 * x + 1], p[x], vi);
+        }
+        ar = fma(ur, p[k], ar);
+        ai = fma(ui, p[k], ai);
+        br += ur * vr - ui * vi;
+        bi_ += ur * vi + ui * vr;
+      }
+    }
+    cr = warp_sum(cr);
+    ci = warp_sum(ci);
+    ar = warp_sum(ar);
+    ai = warp_sum(ai);
+    br = warp_sum(br);
+    bi_ = warp_sum(bi_);
+    if (lane == 0)  // 2 c s1 - s2
+      blk[gl * wpt + wl] = make_double2(2.0 * (cr * ar - ci * ai) - br, 2.0 * (cr * ai + ci * ar) - bi_);
+  }
+  __syncthreads();
+  for (int wl = threadIdx.x; wl < wcount; wl += Cfg::NT) {
+    double sx = 0, sy = 0;
+    for (int gl = 0; gl < gcount; ++gl) {
+      const double2 v = blk[gl * wpt + wl];
+      sx += v.x;
+      sy += v.y;
+    }
+    orbout[2 * ((long long)mt * W + w0 + wl)] = sx;
+    orbout[2 * ((long long)mt * W + w0 + wl) + 1] = sy;
+  }
+}
+
+// Theta (W, N, No) complex: rows p < No set to zero (the occupied block)
+__global__ void theta_zero_occ_kernel(double2* theta, int W, int N, int no) {
+  const long long n = (long long)W * no * no;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long w = e / ((long long)no * no), r = e - w * no * no;
+    theta[w * N * no + r] = make_double2(0.0, 0.0);
+  }
+}
+
+// orbital energy per walker: sum of the row-tile partials (one warp per walker)
+__global__ void orb_combine_kernel(int W, int mt, const double* part, double* out) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= W) return;
+  double xr = 0, xi = 0;
+  for (int m = lane; m < mt; m += 32) {
+    xr += part[2 * ((long long)m * W + w)];
+    xi += part[2 * ((long long)m * W + w) + 1];
+  }
+  xr = warp_sum(xr);
+  xi = warp_sum(xi);
+  if (lane == 0) {
+    out[2LL * w] = xr;
+    out[2LL * w + 1] = xi;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // local energy from the pieces (one warp per walker)
 // ---------------------------------------------------------------------------
 __global__ void energy_combine_kernel(int W, int G, int ns, int restricted, const double* scal,
@@ -447,6 +556,52 @@ cudaError_t launch_exchange(const Layout& L, const double* prep, double* work, i
   if (L.ex[s].bn == 120) return run_exch<CfgX120>(L, prep, work, s, st);
   if (L.ex[s].bn == 160) return run_exch<CfgX160>(L, prep, work, s, st);
   return cudaErrorInvalidValue;
+}
+
+template <class Cfg>
+static cudaError_t run_orb(const Layout& L, const double* prep, double* work, const double* prj,
+                           int nlo, cudaStream_t st) {
+  const ExchTile& X = L.ex[0];
+  const int no = L.no[0];
+  const int mt = (L.G + X.gpt - 1) / X.gpt;
+  F64Operand A{prep + L.p_rc[0], L.Npad, 0, 0, kUnseg};
+  F64Operand B{work + L.w_theta[0], 2 * no, 0, (long long)L.N * 2 * no, 2 * no};
+  const size_t stage = size_t(Cfg::BM) * (Cfg::BN + 2) * sizeof(double) +
+                       size_t(kMaxLo) * 64 * sizeof(double) + size_t(X.gpt) * X.wpt * sizeof(double2);
+  const size_t smem = stage > Cfg::SMEM ? stage : Cfg::SMEM;
+  cudaError_t err = set_smem<Cfg>((const void*)orb_kernel<Cfg>, smem);
+  if (err != cudaSuccess) return err;
+  dim3 grid(mt, (L.W + X.wpt - 1) / X.wpt);
+  ProfScope ps(K_EXCH, st);
+  orb_kernel<Cfg><<<grid, Cfg::NT, smem, st>>>(A, B, L.G, no, L.N, L.W, X.gpt, X.wpt, prj, nlo,
+                                               work + L.w_orb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_orbenergy(const Layout& L, const double* prep, double* work, const double* prj,
+                             int nlo, double* out, cudaStream_t st) {
+  if (nlo < 1 || nlo > kMaxLo || L.no[0] > 64) return cudaErrorInvalidValue;
+  {
+    ProfScope ps(K_MISC, st);
+    theta_zero_occ_kernel<<<256, 256, 0, st>>>(reinterpret_cast<double2*>(work + L.w_theta[0]), L.W,
+                                               L.N, L.no[0]);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (L.ex[0].bn == 80)
+    e = run_orb<CfgX80>(L, prep, work, prj, nlo, st);
+  else if (L.ex[0].bn == 120)
+    e = run_orb<CfgX120>(L, prep, work, prj, nlo, st);
+  else if (L.ex[0].bn == 160)
+    e = run_orb<CfgX160>(L, prep, work, prj, nlo, st);
+  else
+    return cudaErrorInvalidValue;
+  if (e != cudaSuccess) return e;
+  const int wpb = 8;
+  const int mt = (L.G + L.ex[0].gpt - 1) / L.ex[0].gpt;
+  ProfScope ps(K_ECOMB, st);
+  orb_combine_kernel<<<(L.W + wpb - 1) / wpb, 32 * wpb, 0, st>>>(L.W, mt, work + L.w_orb, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_energy_combine(const Layout& L, const double* prep, double* work, double* eout,

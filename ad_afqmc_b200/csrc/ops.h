@@ -47,6 +47,10 @@ cudaError_t launch_propagate_walkers(const Layout& L, const double* prepared, do
                                      cudaStream_t st);
 cudaError_t launch_exchange(const Layout& L, const double* prepared, double* work, int sector,
                             cudaStream_t st);
+// LNO orbital energy of restricted walkers from Theta in the workspace
+// (overwrites its occupied rows); prj: n_lo x No device doubles, n_lo <= 8
+cudaError_t launch_orbenergy(const Layout& L, const double* prepared, double* work,
+                             const double* prj, int nlo, double* out, cudaStream_t st);
 cudaError_t launch_energy_combine(const Layout& L, const double* prepared, double* work,
                                   double* eout, int eout_stride, cudaStream_t st);
 

@@ -72,3 +72,58 @@ def afqmc_energy(ham_data: dict, ham, propagator, trial, wave_data: dict, sample
     np.savetxt(tmpdir + "/samples_raw.dat", np.stack((w, e)).T)
     clean, _ = stat_utils.reject_outliers(np.stack((w, e)).T, 1)
     return stat_utils.blocking_analysis(clean[:, 0], clean[:, 1], neql=0)
+
+
+def afqmc_LNOenergy(ham_data: dict, ham, propagator, trial, wave_data: dict, sampler, options: dict,
+                    MPI=None, init_walkers=None, tmpdir: str = ".",
+                    results: Optional[dict] = None) -> Tuple[float, float]:
+    """driver.afqmc_LNOenergy, driver.py:195-402, on one GPU: equilibration,
+    sampling blocks of a sampler_lno (energy and orbital energy per block),
+    stop when the orbital energy's standard error of the mean drops below
+    options["maxError"] (checked every max(n_blocks // 5, 1) blocks after the
+    fifth, driver.py:376-389), then the analysis of driver.py:1338-1400.
+    Returns (E, E_err) as the reference; ``results`` (optional dict) also
+    receives the orbital energy, its error and the block data."""
+    if "rdm1" not in wave_data:
+        wave_data["rdm1"] = trial.get_rdm1(wave_data)
+    ham_data = ham.build_measurement_intermediates(ham_data, trial, wave_data)
+    ham_data = ham.build_propagation_intermediates(ham_data, propagator, trial, wave_data)
+    prop_data = propagator.init_prop_data(trial, wave_data, ham_data, options.get("seed", 0),
+                                          init_walkers)
+    if float(torch.abs(torch.sum(prop_data["overlaps"]))) < 1.0e-6:
+        raise ValueError("Initial overlaps are zero. Pass walkers with non-zero overlap.")
+    sampler_eq = sampler_cls(n_prop_steps=50, n_ene_blocks=options.get("n_ene_blocks_eql", 1),
+                             n_sr_blocks=options.get("n_sr_blocks_eql", 5),
+                             n_blocks=options.get("n_eql", 1))
+    prop_data = _run_equilibration(ham, ham_data, propagator, prop_data, trial, wave_data, sampler_eq)
+    max_error = options["maxError"]
+    nb = sampler.n_blocks
+    energies, weights, orbes = [], [], []
+    truncate_at = nb
+    for n in range(nb):
+        e, prop_data, o = sampler.propagate_phaseless(ham, ham_data, propagator, prop_data, trial, wave_data)
+        energies.append(float(e))
+        weights.append(float(torch.sum(prop_data["weights"])))
+        orbes.append(float(o))
+        prop_data["walkers"] = prop_data["walkers"].orthonormalize()
+        zeta = prop_data["key"].uniform()
+        prop_data["walkers"], prop_data["weights"] = prop_data["walkers"].stochastic_reconfiguration_global(
+            prop_data["weights"], zeta)
+        prop_data["e_estimate"] = 0.9 * prop_data["e_estimate"] + 0.1 * e
+        if n % max(nb // 5, 1) == 0 and n > 4:
+            sem = np.std(orbes[: n + 1]) / np.sqrt(n + 1)
+            if sem < max_error:
+                truncate_at = n
+                break
+    w = np.array(weights[: truncate_at + 1])
+    e = np.array(energies[: truncate_at + 1])
+    o = np.array(orbes[: truncate_at + 1])
+    np.savetxt(tmpdir + "/samples_raw.dat", np.stack((w, e)).T)
+    clean, _ = stat_utils.reject_outliers(np.stack((w, e)).T, 1)
+    e_afqmc, e_err = stat_utils.blocking_analysis(clean[:, 0], clean[:, 1], neql=0)
+    orbe, orbe_err = stat_utils.blocking_analysis(w, o, neql=0)
+    if results is not None:
+        results.update({"orbE": orbe, "orbE_err": orbe_err if orbe_err is not None else 0.0,
+                        "block_energies": e, "block_weights": w, "block_orbEs": o,
+                        "n_blocks": len(e)})
+    return e_afqmc, e_err

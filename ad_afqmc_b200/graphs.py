@@ -35,12 +35,14 @@ from .walkers import UHFWalkers
 
 class BlockGraph:
     def __init__(self, ham, ham_data, prop, trial, wave_data, prop_data, n_prop_steps: int = 10,
-                 update_estimate: bool = True, reconfigure: bool = True):
+                 update_estimate: bool = True, reconfigure: bool = True, lno: bool = False):
         """reconfigure=False leaves the comb (and the overlaps of the new
         walkers) out of the recorded block, for callers that reconfigure
         across ranks after each replay; update_estimate=False leaves out the
         e_estimate update (a caller with several ranks updates it from the
-        all-reduced block energy)."""
+        all-reduced block energy).  lno=True records the block end of
+        sampler_lno (sampling.py:586-631) for an rhf_lno trial and restricted
+        walkers: block_out then holds (energy, weight, orbital energy)."""
         self.prop, self.trial, self.wave_data, self.ham_data = prop, trial, wave_data, ham_data
         self.eng = prop.engine(ham_data, trial, wave_data)
         if not self.eng.has_prop:
@@ -61,7 +63,15 @@ class BlockGraph:
         self.seed = key.seed
         self.counter = torch.tensor([key.counter], dtype=torch.int64, device=dev)
         self.zeta = torch.zeros(1, dtype=torch.float64, device=dev)
-        self.block_out = torch.zeros(2, dtype=torch.float64, device=dev)
+        self.lno = bool(lno)
+        self.block_out = torch.zeros(3 if self.lno else 2, dtype=torch.float64, device=dev)
+        if self.lno:
+            if isinstance(w, UHFWalkers) or "prjlo" not in wave_data:
+                raise _lib.AfqError("the LNO block needs restricted walkers and wave_data['prjlo']")
+            self.prj = torch.as_tensor(wave_data["prjlo"], dtype=torch.float64, device=dev).reshape(
+                -1, trial.nelec[0]).contiguous()
+            self.e_buf = torch.empty(W, dtype=torch.complex128, device=dev)
+            self.o_buf = torch.empty(W, dtype=torch.complex128, device=dev)
         self.w_tmp = torch.empty_like(prop_data["weights"])
         self.idx = torch.empty(W, dtype=torch.int32, device=dev)
         self.small = torch.empty(W * 16, dtype=torch.float64, device=dev)  # own: solves may overlap
@@ -86,8 +96,11 @@ class BlockGraph:
             _lib.check(lib.afq_propagate_constrained(C.byref(eng.dims), p, C.byref(st),
                                                      self.fields[s].data_ptr(), w, wb, stream),
                        "afq_propagate_constrained")
-        _lib.check(lib.afq_block_end(C.byref(eng.dims), p, C.byref(st), self.block_out.data_ptr(), w,
-                                     wb, stream), "afq_block_end")
+        if self.lno:
+            self._lno_block_end(lib, stream)
+        else:
+            _lib.check(lib.afq_block_end(C.byref(eng.dims), p, C.byref(st), self.block_out.data_ptr(),
+                                         w, wb, stream), "afq_block_end")
         if not self.reconfigure:
             sc[2].div_(self.prop.n_walkers)
             if self.update_estimate:
@@ -114,6 +127,39 @@ class BlockGraph:
             sc[0].mul_(0.9).add_(0.1 * self.block_out[0])
         self.launches_per_block = _lib.launch_count() - n0
         pd.pop("_afq_green_of", None)
+
+    def _lno_block_end(self, lib, stream) -> None:
+        """sampler_lno._block_scan after the steps (sampling.py:586-631): QR,
+        overlaps, local and orbital energies on the propagator's engine, the
+        reference's clamps against pop_control_ene_shift, block averages and
+        the shift update; device work only, so it records into the graph."""
+        pd, eng = self.pd, self.eng
+        sc = pd["_scalars"]
+        p, w, wb = eng.handle
+        wts = pd["weights"]
+        sc[2].add_(wts.numel() - torch.count_nonzero(wts).to(torch.float64))
+        win = _lib.pair(self.tensors[0].data_ptr(), None)
+        _lib.check(lib.afq_orthonormalize(C.byref(eng.dims), win, None, self.small.data_ptr(),
+                                          self.small.numel() * 8, stream), "afq_orthonormalize")
+        mo = _lib.pair(self.mo[0].data_ptr(), self.mo[-1].data_ptr())
+        _lib.check(lib.afq_calc_overlap(C.byref(eng.dims), mo, win, pd["overlaps"].data_ptr(),
+                                        self.small.data_ptr(), self.small.numel() * 8, stream),
+                   "afq_calc_overlap")
+        _lib.check(lib.afq_calc_energy(C.byref(eng.dims), p, win, self.e_buf.data_ptr(), w, wb, stream),
+                   "afq_calc_energy")
+        _lib.check(lib.afq_calc_orbenergy(C.byref(eng.dims), p, win, self.prj.data_ptr(),
+                                          int(self.prj.shape[0]), self.o_buf.data_ptr(), w, wb, stream),
+                   "afq_calc_orbenergy")
+        lim = (2.0 / self.prop.dt) ** 0.5
+        shift = sc[1].clone()
+        e = torch.real(self.e_buf)
+        e = torch.where(torch.abs(e - shift) > lim, shift, e)
+        o = torch.where(torch.abs(e - shift) > lim, shift, torch.real(self.o_buf))
+        bw = torch.sum(wts)
+        self.block_out[0] = torch.sum(e * wts) / bw
+        self.block_out[1] = bw
+        self.block_out[2] = torch.sum(o * wts) / bw
+        sc[1].copy_(0.9 * shift + 0.1 * self.block_out[0])
 
     # -- capture / replay ----------------------------------------------------
     def capture(self, warmup: int = 1, device_sync: bool = True) -> "BlockGraph":

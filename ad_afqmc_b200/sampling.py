@@ -93,3 +93,73 @@ class sampler:
 
     def __hash__(self) -> int:
         return hash((self.n_prop_steps, self.n_ene_blocks, self.n_sr_blocks, self.n_blocks))
+
+
+@dataclass
+class sampler_lno(sampler):
+    """sampling.sampler_lno (sampling.py:583-694): every energy block also
+    averages the fragment's orbital energy (trial.calc_orbenergy, an rhf_lno
+    trial).  Its block end clamps the local energies against
+    pop_control_ene_shift (not e_estimate), and the orbital energies where the
+    already clamped energies are still out of range, which never happens: both
+    as the reference does.  propagate_phaseless returns (E, prop_data, orbE)."""
+
+    def _block_scan(self, prop, trial, ham_data, prop_data, wave_data, out_row):
+        """sampling.py:586-631."""
+        eng = prop.engine(ham_data, trial, wave_data)
+        nchol = int(ham_data["chol"].shape[0])
+        fields = self._fields(prop, prop_data, nchol)
+        p, w, wb = eng.handle
+        lib = _lib.lib()
+        stream = _lib.stream_handle()
+        st = make_state(prop_data, eng)
+        for s in range(self.n_prop_steps):
+            _lib.check(lib.afq_propagate_constrained(C.byref(eng.dims), p, C.byref(st),
+                                                     fields[s].data_ptr(), w, wb, stream),
+                       "afq_propagate_constrained")
+        note_state(prop_data, st, eng)
+        sc = prop_data["_scalars"]
+        wts = prop_data["weights"]
+        sc[2].add_(wts.numel() - torch.count_nonzero(wts).to(torch.float64))
+        prop_data["walkers"] = prop_data["walkers"].orthonormalize()
+        prop_data.pop("_afq_green_of", None)
+        prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+        lim = (2.0 / prop.dt) ** 0.5
+        shift = sc[1].clone()
+        e = torch.real(trial.calc_energy(prop_data["walkers"], ham_data, wave_data, engine=eng))
+        e = torch.where(torch.abs(e - shift) > lim, shift, e)
+        o = torch.real(trial.calc_orbenergy(prop_data["walkers"], ham_data, wave_data, engine=eng))
+        o = torch.where(torch.abs(e - shift) > lim, shift, o)
+        bw = torch.sum(wts)
+        out_row[0] = torch.sum(e * wts) / bw
+        out_row[1] = bw
+        out_row[2] = torch.sum(o * wts) / bw
+        sc[1].copy_(0.9 * shift + 0.1 * out_row[0])
+
+    def propagate_phaseless(self, ham, ham_data: dict, prop, prop_data: dict, trial, wave_data: dict):
+        """sampling.py:663-689."""
+        eng = prop.engine(ham_data, trial, wave_data)
+        if not eng.has_prop:
+            raise _lib.AfqError("propagation intermediates missing: call build_propagation_intermediates")
+        prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+        prop_data["n_killed_walkers"] = 0.0
+        prop_data["pop_control_ene_shift"] = prop_data["e_estimate"]
+        if isinstance(prop_data["pop_control_ene_shift"], torch.Tensor):
+            prop_data["pop_control_ene_shift"] = prop_data["pop_control_ene_shift"].clone()
+        sync_scalars(prop_data)
+        nb = self.n_sr_blocks * self.n_ene_blocks
+        out = torch.zeros(nb, 3, dtype=torch.float64, device=device())
+        i = 0
+        for _ in range(self.n_sr_blocks):
+            for _ in range(self.n_ene_blocks):
+                self._block_scan(prop, trial, ham_data, prop_data, wave_data, out[i])
+                i += 1
+            zeta = self._uniform(prop_data)
+            prop_data["walkers"], prop_data["weights"] = prop_data[
+                "walkers"].stochastic_reconfiguration_local(prop_data["weights"], zeta)
+            prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+        sc = prop_data["_scalars"]
+        sc[2].div_(nb * prop.n_walkers)
+        be, bw, bo = out[:, 0], out[:, 1], out[:, 2]
+        prop_data["block_energies"] = out
+        return torch.sum(be * bw) / torch.sum(bw), prop_data, torch.sum(bo * bw) / torch.sum(bw)

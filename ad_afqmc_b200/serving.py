@@ -60,6 +60,7 @@ class Request:
     n_walkers: int
     seed: int
     arrival: float = 0.0          # seconds from the start of the run
+    prjlo: Optional[np.ndarray] = None  # (n_lo, nocc): an LNO fragment (orbital energy, rhf_lno)
 
 
 @dataclass
@@ -74,6 +75,8 @@ class Result:
     started: float                # first block launched (setup done)
     finished: float
     block_energies: List[float] = field(default_factory=list)
+    orbE: Optional[float] = None        # LNO fragments: orbital energy and its error
+    orbE_err: Optional[float] = None
 
     @property
     def latency(self) -> float:
@@ -112,21 +115,25 @@ class Solve:
         self.t_admit = t_admit
         self.t_start = 0.0
         self.stream = stream if stream is not None else torch.cuda.Stream()
-        self.host = torch.empty(2, dtype=torch.float64).pin_memory()
+        self.lno = req.prjlo is not None
+        self.host = torch.empty(3, dtype=torch.float64).pin_memory()
         self.event = torch.cuda.Event()
         sys_ = req.system
         with torch.cuda.stream(self.stream):
-            trial = wavefunctions.rhf(sys_.norb, sys_.nelec)
+            trial = (wavefunctions.rhf_lno if self.lno else wavefunctions.rhf)(sys_.norb, sys_.nelec)
             ham = hamiltonian.hamiltonian(sys_.norb)
             prop = propagation.propagator_afqmc(dt=0.005, n_walkers=req.n_walkers, precision=precision)
             hd, wd = sys_.ham_data(), sys_.wave_data()
+            if self.lno:
+                wd["prjlo"] = np.asarray(req.prjlo, dtype=np.float64)
             hd = ham.build_measurement_intermediates(hd, trial, wd)
             hd = ham.build_propagation_intermediates(hd, prop, trial, wd)
             pd = prop.init_prop_data(trial, wd, hd, seed=req.seed)
-            self.block = BlockGraph(ham, hd, prop, trial, wd, pd, n_prop_steps=n_prop_steps)
+            self.block = BlockGraph(ham, hd, prop, trial, wd, pd, n_prop_steps=n_prop_steps, lno=self.lno)
             self.block.capture(warmup=0, device_sync=False)
         self.energies: List[float] = []
         self.weights: List[float] = []
+        self.orbes: List[float] = []
         self.n_done = 0
         self.in_flight = False
 
@@ -137,7 +144,7 @@ class Solve:
             for _ in range(n_eql):
                 self.block.replay()
             out = self.block.replay()
-            self.host.copy_(out, non_blocking=True)
+            self.host[: out.numel()].copy_(out, non_blocking=True)
             self.event.record(self.stream)
         self.in_flight = True
 
@@ -148,6 +155,8 @@ class Solve:
         self.in_flight = False
         self.energies.append(float(self.host[0]))
         self.weights.append(float(self.host[1]))
+        if self.lno:
+            self.orbes.append(float(self.host[2]))
         return True
 
     def blocking_error(self) -> Optional[float]:
@@ -194,10 +203,13 @@ class Server:
         return self._streams
 
     def _done(self, s: Solve) -> Tuple[bool, Optional[float], bool]:
-        """(stop, error, converged) after the block just read."""
+        """(stop, error, converged) after the block just read.  LNO fragments
+        stop on their orbital energies (driver.py:376-389), others on the
+        block energies."""
         n = len(s.energies)
         if self.stop_rule == "sem":
-            conv, err = sem_stop(np.array(s.energies), self.max_blocks, self.target_error)
+            series = s.orbes if s.lno else s.energies
+            conv, err = sem_stop(np.array(series), self.max_blocks, self.target_error)
         else:
             err = s.blocking_error() if n >= self.min_blocks else None
             conv = err is not None and err < self.target_error
@@ -259,8 +271,13 @@ class Server:
                         en = float(np.sum(e[ok] * w[ok]) / np.sum(w[ok])) if ok.any() else float("nan")
                         if err is None:
                             err = float(np.std(e) / np.sqrt(len(e))) if len(e) > 1 else None
-                        results.append(Result(s.req.rid, en, err, len(e), conv, s.req.arrival, s.t_admit,
-                                              s.t_start, clock(), list(s.energies)))
+                        res = Result(s.req.rid, en, err, len(e), conv, s.req.arrival, s.t_admit,
+                                     s.t_start, clock(), list(s.energies))
+                        if s.lno:
+                            o = np.array(s.orbes)
+                            res.orbE = float(np.sum(o[ok] * w[ok]) / np.sum(w[ok])) if ok.any() else float("nan")
+                            res.orbE_err = float(np.std(o) / np.sqrt(len(o))) if len(o) > 1 else None
+                        results.append(res)
                         active.remove(s)
                         used -= sizes.pop(s.req.rid)
                         free_streams.append(slot_of.pop(s.req.rid))
@@ -279,7 +296,8 @@ class Server:
 
 
 def make_requests(rate: float, duration: float, seed: int = 1005, large_frac: float = 0.10,
-                  chol_scale: Optional[float] = None, pinned: bool = True) -> List[Request]:
+                  chol_scale: Optional[float] = None, pinned: bool = True,
+                  lno: bool = False) -> List[Request]:
     """Poisson arrivals at ``rate``/s for ``duration`` s. Sizes follow the uneven
     fragment batch, plus ``large_frac`` of them at N=250, G=1250. The two-body
     scale is ``fragment_chol_scale(N)`` unless ``chol_scale`` is given. With
@@ -298,7 +316,11 @@ def make_requests(rate: float, duration: float, seed: int = 1005, large_frac: fl
         sys_ = make_system(sp["norb"], tuple(sp["nelec"]), sp["nchol"], sp["seed"], "rhf", chol_scale=cs)
         if pinned:
             sys_.pin()
-        out.append(Request(i, sys_, sp["n_walkers"], sp["seed"], a))
+        prj = None
+        if lno:  # one localized orbital per fragment, a normalized row (lnoafqmc.py:147)
+            prj = rng.standard_normal((1, sp["nelec"][0]))
+            prj /= np.linalg.norm(prj)
+        out.append(Request(i, sys_, sp["n_walkers"], sp["seed"], a, prj))
     return out
 
 
@@ -332,12 +354,14 @@ def main():
     ap.add_argument("--slots", type=int, default=16)
     ap.add_argument("--stop-rule", default="sem", choices=["sem", "blocking"])
     ap.add_argument("--no-baseline", action="store_true")
+    ap.add_argument("--lno", action="store_true",
+                    help="LNO fragments: orbital energies (rhf_lno), stop on their standard error")
     a = ap.parse_args()
     torch.cuda.set_device(0)
-    reqs = make_requests(a.rate, a.duration)
+    reqs = make_requests(a.rate, a.duration, lno=a.lno)
     srv = Server(a.precision, max_slots=a.slots, max_blocks=a.max_blocks, stop_rule=a.stop_rule)
     # warm the CUDA context and kernels with throw-away requests of every path
-    warm = make_requests(4.0, 1.0, seed=7)[:3]
+    warm = make_requests(4.0, 1.0, seed=7, lno=a.lno)[:3]
     srv.run(warm, realtime=False)
     one_by_one(warm[:1], srv)
     t0 = time.perf_counter()
@@ -346,7 +370,7 @@ def main():
     out = {"workload": (f"Poisson {a.rate}/s for {a.duration} s: N~U[30,160], No=round(N/4), G~U[4N,6N], "
                         f"W~U[64,256], 10% N=250/G=1250; stop std err < 0.5 mHa ({a.stop_rule}) "
                         f"or {a.max_blocks} blocks after 5 equilibration blocks"),
-           "precision": a.precision, "slots": a.slots, "serving": summarize(res, wall)}
+           "precision": a.precision, "slots": a.slots, "lno": a.lno, "serving": summarize(res, wall)}
     if not a.no_baseline:
         t0 = time.perf_counter()
         base = one_by_one(reqs, srv)

@@ -194,6 +194,29 @@ class rhf(wave_function):
 
 
 @dataclass
+
+class rhf_lno(rhf):
+    """RHF trial of an LNO fragment (wavefunctions.py:6871-6926): the rhf
+    measurements plus the orbital energy of the fragment's localized orbital,
+    whose projector is wave_data["prjlo"] ((n_lo, nocc), lnoafqmc.py:147)."""
+
+    def calc_orbenergy(self, walkers: walker_batch, ham_data: dict, wave_data: dict, *,
+                       engine=None) -> torch.Tensor:
+        """wavefunctions.py:6898-6923 -> afq_calc_orbenergy (W,) complex128."""
+        if not isinstance(walkers, RHFWalkers):
+            raise NotImplementedError("Walker type not supported")  # as the reference
+        eng = engine if engine is not None else get_engine(ham_data, self, wave_data, "restricted",
+                                                           walkers.n_walkers)
+        prj = to_dev(wave_data["prjlo"], torch.float64).reshape(-1, self.nelec[0]).contiguous()
+        out = torch.empty(walkers.n_walkers, dtype=torch.complex128, device=eng.prepared.device)
+        p, w, wb = eng.handle
+        _lib.check(
+            _lib.lib().afq_calc_orbenergy(C.byref(eng.dims), p, _ptrs(walkers), prj.data_ptr(),
+                                          int(prj.shape[0]), out.data_ptr(), w, wb, _lib.stream_handle()),
+            "afq_calc_orbenergy",
+        )
+        return out
+
 class uhf(wave_function):
     """Unrestricted Hartree-Fock trial (wavefunctions.py:1238-1499)."""
 

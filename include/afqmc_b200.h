@@ -188,6 +188,16 @@ int afq_stochastic_reconfiguration(const afq_dims* d, const double* weights_in, 
                                    double* const walkers_out[2], double* weights_out,
                                    int32_t* indices, void* stream);
 
+/* Orbital energy of an LNO fragment's localized orbital for restricted
+ * walkers and an RHF trial: rhf_lno._calc_orbenergy (wavefunctions.py:
+ * 6898-6923), with f_g = rot_chol[g][:, No:] G^T[No:, :] (virtual block),
+ * m = prjlo^T prjlo, orbE = 2 sum_g tr(f_g) sum(f_g o m) - sum_g sum((f_g f_g) o m).
+ * prjlo: (n_lo, No) device doubles, 1 <= n_lo <= 8.  orbe: (W,) complex128.
+ * FP64 whatever the precision of dims; f is never written to memory. */
+int afq_calc_orbenergy(const afq_dims* d, const void* prepared, const double* const walkers[2],
+                       const double* prjlo, int32_t n_lo, double* orbe, void* work,
+                       size_t work_bytes, void* stream);
+
 /* Comb of the reconfiguration across ranks: weights_all holds the weights
  * of n_ranks ranks of n_per_rank walkers each, in rank order (an all-gather).
  * Writes, for every one of the n_ranks * n_per_rank slots, the global index of

@@ -91,6 +91,23 @@ class RHFTrial:
         ene2 = 2.0 * np.sum(c * c) - exc
         return ene2 + ene1 + h0
 
+    def orbenergy_restricted(self, walker, ham_data, wave_data):
+        """rhf_lno._calc_orbenergy, wavefunctions.py:6904-6923: orbital energy of
+        the fragment's localized orbital (projector prjlo, (n_lo, nocc)).  f is
+        rot_chol's virtual columns times the virtual rows of G^T."""
+        rot_h1, rot_chol = ham_data["rot_h1"], ham_data["rot_chol"]
+        m = np.asarray(wave_data["prjlo"]).T @ np.asarray(wave_data["prjlo"])
+        nocc = rot_h1.shape[0]
+        g = green(walker, wave_data["mo_coeff"])
+        f = np.einsum("gij,jk->gik", rot_chol[:, :nocc, nocc:], g.T[nocc:, :nocc], optimize=True)
+        c = np.einsum("gii->g", f)
+        j2 = np.einsum("Gxk,xk,G->", f, m, c, optimize=True) * 2
+        x2 = np.einsum("Gxy,Gyk,xk->", f, f, m, optimize=True)
+        return j2 - x2
+
+    def calc_orbenergy(self, walkers, ham_data, wave_data):
+        return np.array([self.orbenergy_restricted(w, ham_data, wave_data) for w in walkers])
+
     def energy_unrestricted(self, wu, wd, ham_data, wave_data):
         """wavefunctions.py:1143-1174."""
         h0, rot_h1, rot_chol = ham_data["h0"], ham_data["rot_h1"], ham_data["rot_chol"]
@@ -559,6 +576,44 @@ class Sampler:
         be, bw = np.array(be), np.array(bw)
         prop_data["n_killed_walkers"] /= self.n_sr_blocks * self.n_ene_blocks * prop.n_walkers
         return np.sum(be * bw) / np.sum(bw), prop_data
+
+
+class SamplerLNO(Sampler):
+    """sampling.sampler_lno, sampling.py:583-694: blocks also average the
+    orbital energy; both samples are clamped against pop_control_ene_shift
+    (the orbital energy where the total energy is clamped)."""
+
+    def block_scan(self, prop, trial, ham_data, prop_data, wave_data, rnd):
+        """sampling.py:586-631."""
+        n_chol = np.asarray(ham_data["chol"]).shape[0]
+        fields = rnd.fields(self.n_prop_steps, prop.n_walkers, n_chol)
+        for s in range(self.n_prop_steps):
+            prop_data = prop.propagate_constrained(trial, ham_data, prop_data, fields[s], wave_data)
+        prop_data["n_killed_walkers"] += prop_data["weights"].size - np.count_nonzero(
+            prop_data["weights"]
+        )
+        prop_data["walkers"] = orthonormalize(prop_data["walkers"])
+        prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+        e = np.real(trial.calc_energy(prop_data["walkers"], ham_data, wave_data))
+        shift = prop_data["pop_control_ene_shift"]
+        clamp = np.abs(e - shift) > np.sqrt(2.0 / prop.dt)
+        e = np.where(clamp, shift, e)
+        o = np.real(trial.calc_orbenergy(prop_data["walkers"], ham_data, wave_data))
+        o = np.where(np.abs(e - shift) > np.sqrt(2.0 / prop.dt), shift, o)
+        block_weight = np.sum(prop_data["weights"])
+        block_energy = np.sum(e * prop_data["weights"]) / block_weight
+        block_orbe = np.sum(o * prop_data["weights"]) / block_weight
+        prop_data["pop_control_ene_shift"] = 0.9 * shift + 0.1 * block_energy
+        self._orbe.append((block_orbe, block_weight))
+        return prop_data, (block_energy, block_weight)
+
+    def propagate_phaseless(self, prop, trial, ham_data, prop_data, wave_data, rnd):
+        """sampling.py:663-689: (energy, prop_data, orbital energy)."""
+        self._orbe = []
+        e, prop_data = super().propagate_phaseless(prop, trial, ham_data, prop_data, wave_data, rnd)
+        o = np.array([x[0] for x in self._orbe])
+        w = np.array([x[1] for x in self._orbe])
+        return e, prop_data, np.sum(o * w) / np.sum(w)
 
 
 def afqmc_blocks(prop, trial, ham_data, prop_data, wave_data, sampler, rnd, n_blocks):

@@ -65,3 +65,24 @@ def test_stop_rule_ends_converged_solves_early():
     res = Server("mixed", n_prop_steps=3, n_eql=1, max_blocks=30, target_error=10.0, stop_rule="blocking",
                  min_blocks=5).run(reqs, realtime=False)
     assert all(r.converged and r.n_blocks == 5 for r in res)
+
+
+def test_lno_fragments_served_identically_alone_and_in_the_mix():
+    """LNO fragments (rhf_lno, orbital energy per block): same block and
+    orbital energies alone and in the mix; the orbital energy is reported."""
+    from ad_afqmc_b200.serving import Request, Server
+
+    reqs = _requests()
+    rng = np.random.default_rng(17)
+    for r in reqs:
+        p = rng.standard_normal((1, r.system.nelec[0]))
+        r.prjlo = p / np.linalg.norm(p)
+    srv = Server("mixed", n_prop_steps=3, n_eql=1, max_blocks=4, target_error=-1.0)
+    mixed = {r.rid: r for r in srv.run(reqs, realtime=False)}
+    one = Server("mixed", max_slots=1, n_prop_steps=3, n_eql=1, max_blocks=4, target_error=-1.0,
+                 setup_thread=False)
+    for req in reqs[:2]:
+        alone = one.run([req], realtime=False)[0]
+        assert alone.block_energies == mixed[req.rid].block_energies
+        assert alone.orbE == mixed[req.rid].orbE
+        assert np.isfinite(alone.orbE) and alone.orbE_err is not None
