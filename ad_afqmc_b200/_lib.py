@@ -76,10 +76,12 @@ class afq_tuning(C.Structure):
         ("f64_exch_bn", C.c_int32),
         ("max_stages", C.c_int32),
         ("grid_cap", C.c_int32),
-        ("reserved", C.c_int32 * 9),
+        ("prop_epi_groups", C.c_int32),
+        ("reserved", C.c_int32 * 8),
     ]
 
-    KNOBS = ("fb_splitk", "fb_bn", "vhs_bn", "exch_bn", "f64_exch_bn", "max_stages", "grid_cap")
+    KNOBS = ("fb_splitk", "fb_bn", "vhs_bn", "exch_bn", "f64_exch_bn", "max_stages", "grid_cap",
+             "prop_epi_groups")
 
     def as_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k in self.KNOBS}

@@ -188,7 +188,7 @@ int afq_gemm_split_bf16(const void* const a_pieces[3], int npa, const void* cons
   P.epi.bstride = c_bstride;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   ProfScope ps(K_MISC, st);
-  if (launch_umma<BN>(P, 0, num_sms(), st) != cudaSuccess) return AFQ_ERR_CUDA;
+  if (launch_umma<BN>(P, num_sms(), st) != cudaSuccess) return AFQ_ERR_CUDA;
   return AFQ_OK;
 }
 

@@ -416,21 +416,25 @@ void base_shape(UmmaParams<Epi>& P, int npc, int M, int N, int K, int batch, int
   P.s.err = err;
 }
 
-template <int BN, class Epi>
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// `extra`: epilogue scratch bytes per epilogue warpgroup
+template <int BN, int EG = 1, class Epi>
 int run(UmmaParams<Epi>& P, size_t extra, cudaStream_t st, int prof_id, const afq_tuning& T) {
-  P.s.stages = umma_pick_stages(BN, P.s.npa, P.s.npb, extra);
+  P.s.epi_bytes = (int)align256(extra);
+  P.s.stages = umma_pick_stages(BN, P.s.npa, P.s.npb, size_t(EG) * P.s.epi_bytes);
   if (P.s.stages < 2 && P.s.kc > 0 && extra == umma_chunk_stage_bytes(BN)) {
     // no room for the chunk staging next to two stages: accumulate in one chunk
     P.s.kc = 0;
-    extra = 0;
-    P.s.stages = umma_pick_stages(BN, P.s.npa, P.s.npb, extra);
+    P.s.epi_bytes = 0;
+    P.s.stages = umma_pick_stages(BN, P.s.npa, P.s.npb, 0);
   }
   if (P.s.stages < 2) return AFQ_ERR_SHAPE;
   if (T.max_stages >= 2 && P.s.stages > T.max_stages) P.s.stages = T.max_stages;
   int ctas = sm_count();
   if (T.grid_cap > 0 && T.grid_cap < ctas) ctas = T.grid_cap;
   ProfScope ps(prof_id, st);
-  return launch_umma<BN>(P, extra, ctas, st) == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
+  return launch_umma<BN, EG>(P, ctas, st) == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
 }
 
 int* err_flag(const Layout& L, double* work) {
@@ -463,7 +467,12 @@ int prop_launch(const Layout& L, const double* prep, double* work, int s, int nc
   P.epi.wout = wout;
   P.s.ngroups = 2;
   P.s.kc = 4;
-  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
+  // the propagator's epilogue (FP32 accumulator update, next operand pieces)
+  // outlasts its MMAs: two epilogue warpgroups when their staging fits
+  if (L.tune.prop_epi_groups != 1 &&
+      umma_pick_stages(BN, L.npc, L.npc, 2 * align256(umma_chunk_stage_bytes(BN))) >= 2)
+    return run<BN, 2>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
+  return run<BN, 1>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
 }
 
 template <int BN>

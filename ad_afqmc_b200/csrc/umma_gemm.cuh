@@ -6,12 +6,16 @@
 // {(0,0),(0,1),(1,0)} is the "BF16x3" product (about 16 significant bits),
 // {(0,0),(0,1),(1,0),(0,2),(1,1),(2,0)} with three pieces about 24 bits.
 //
-// Roles (192 threads, one CTA per SM, persistent over tiles):
+// Roles (64 + 128*EG threads, one CTA per SM, persistent over tiles):
 //   warp 0      TMA producer: 128-byte-swizzled K-major tiles into a STAGES ring
 //   warp 1      TMEM allocator; lane 0 issues tcgen05.mma into one of two
 //               accumulators and commits stage/accumulator barriers
 //   warps 2..5  epilogue: tcgen05.ld rows of the finished accumulator (one TMEM
 //               lane per thread) and hand 32 columns at a time to the functor
+//   warps 6..9  (EG = 2) a second epilogue warpgroup.  The CTA's tiles then
+//               alternate between the groups, tile t in accumulator t & 1 for all
+//               its K chunks, so a long epilogue of one tile runs while the
+//               other group drains and processes the next tile
 // All waits are bounded; on timeout the CTA records an error and unwinds.
 #pragma once
 
@@ -36,6 +40,7 @@ struct UmmaShape {
   int pa[6], pb[6];
   int ngroups;       // 1, or 2: pair 0 (the hi x hi product) accumulates apart from the rest
   int kc;            // K blocks per accumulator chunk (0: the whole K of a tile in one chunk)
+  int epi_bytes;     // epilogue scratch per epilogue warpgroup (bytes, multiple of 256)
   int* err;          // device error flag (set to 1 on a timed-out wait)
 };
 
@@ -93,8 +98,10 @@ inline int umma_pick_stages(int bn, int npa, int npb, size_t extra) {
   return 0;
 }
 
-template <int BN, class Epi>
-__global__ void __launch_bounds__(192, 1) umma_gemm_kernel(const __grid_constant__ UmmaParams<Epi> P) {
+template <int BN, class Epi, int EG>
+__global__ void __launch_bounds__(64 + 128 * EG, 1)
+    umma_gemm_kernel(const __grid_constant__ UmmaParams<Epi> P) {
+  static_assert(EG == 1 || EG == 2, "one or two epilogue warpgroups");
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M=128");
   static_assert(umma_tmem_cols(BN) <= 512, "two accumulators must fit in TMEM");
   extern __shared__ uint8_t smem_raw[];
@@ -176,15 +183,16 @@ __global__ void __launch_bounds__(192, 1) umma_gemm_kernel(const __grid_constant
       constexpr uint32_t idesc = instr_desc(kUBM, BN, 1);
       int stage = 0;
       uint32_t phase = 0;
-      int it = 0;
-      for (int tile = blockIdx.x; tile < tiles && !*abort_s; tile += gridDim.x) {
+      int it = 0, t = 0;
+      uint32_t uses[2] = {0u, 0u};  // EG = 2: chunks accumulated so far in each buffer
+      for (int tile = blockIdx.x; tile < tiles && !*abort_s; tile += gridDim.x, ++t) {
         const int k0 = ((tile / (S.nt * S.mt)) % S.ksplit) * S.kchunk;
         const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
         const int kc = S.kc > 0 ? S.kc : KB;
         bool ok = true;
         for (int c0 = 0; c0 < KB && ok; c0 += kc, ++it) {
-          const int buf = it & 1;
-          const uint32_t use = (uint32_t)(it >> 1);
+          const int buf = EG == 2 ? (t & 1) : (it & 1);
+          const uint32_t use = EG == 2 ? uses[buf]++ : (uint32_t)(it >> 1);
           if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); ok = false; break; }
           tc_fence_after();
           const uint32_t dt = tbase + buf * acc_stride;
@@ -216,11 +224,15 @@ __global__ void __launch_bounds__(192, 1) umma_gemm_kernel(const __grid_constant
     }
   } else {
     const int sub = warp & 3;
+    const int eg = (warp - 2) >> 2;  // epilogue warpgroup
     const int row = sub * 32 + lane;
-    float* srow = reinterpret_cast<float*>(epi_smem) + row * (BN + 1);
-    int it = 0;
+    uint8_t* escr = epi_smem + eg * S.epi_bytes;
+    float* srow = reinterpret_cast<float*>(escr) + row * (BN + 1);
+    int it = 0, t = 0;
+    uint32_t uses = 0;  // EG = 2: chunks drained from this group's buffer so far
     bool ok = true;
-    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++t) {
+      if (EG == 2 && (t & 1) != eg) continue;
       const int nti = tile % S.nt, rest = tile / S.nt;
       const int mti = rest % S.mt, z = rest / S.mt;
       const int k0 = (z % S.ksplit) * S.kchunk;
@@ -228,15 +240,15 @@ __global__ void __launch_bounds__(192, 1) umma_gemm_kernel(const __grid_constant
       const int kc = S.kc > 0 ? S.kc : KB;
       const int nch = (KB + kc - 1) / kc;
       for (int ch = 0; ch < nch; ++ch, ++it) {
-        const int buf = it & 1;
-        const uint32_t use = (uint32_t)(it >> 1);
+        const int buf = EG == 2 ? eg : (it & 1);
+        const uint32_t use = EG == 2 ? uses++ : (uint32_t)(it >> 1);
         if (!mbar_wait_abortable(&accf[buf], use & 1, abort_s)) { fail(); ok = false; break; }
         tc_fence_after();
         const uint32_t taddr = tbase + ((uint32_t)(sub * 32) << 16) + buf * acc_stride;
         if (nch == 1) {
           // z = batch * ksplit + split
           P.epi.template tile<BN>(z, mti, nti, row, AccSrc{taddr, S.ngroups, BN, nullptr}, S,
-                                  epi_smem);
+                                  escr);
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&acce[buf]);
@@ -253,7 +265,7 @@ __global__ void __launch_bounds__(192, 1) umma_gemm_kernel(const __grid_constant
           __syncwarp();
           if (lane == 0) mbar_arrive(&acce[buf]);
           if (ch == nch - 1)
-            P.epi.template tile<BN>(z, mti, nti, row, AccSrc{0u, 1, BN, srow}, S, epi_smem);
+            P.epi.template tile<BN>(z, mti, nti, row, AccSrc{0u, 1, BN, srow}, S, escr);
         }
       }
     }
@@ -274,17 +286,17 @@ int make_tmap_bf16(CUtensorMap* map, const void* base, long long K, long long ro
                    long long batch, long long row_stride_elems, long long batch_stride_elems,
                    int box_rows);
 
-// P.s.stages must come from umma_pick_stages(BN, npa, npb, epi_extra).
-template <int BN, class Epi>
-cudaError_t launch_umma(const UmmaParams<Epi>& P, size_t epi_extra, int num_sms, cudaStream_t st) {
-  const size_t smem = umma_smem_bytes(BN, P.s.stages, P.s.npa, P.s.npb, epi_extra);
-  if (P.s.stages < 2 || smem > kUmmaSmemBudget) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(umma_gemm_kernel<BN, Epi>,
+// P.s.stages must come from umma_pick_stages(BN, npa, npb, EG * P.s.epi_bytes).
+template <int BN, int EG = 1, class Epi>
+cudaError_t launch_umma(const UmmaParams<Epi>& P, int num_sms, cudaStream_t st) {
+  const size_t smem = umma_smem_bytes(BN, P.s.stages, P.s.npa, P.s.npb, size_t(EG) * P.s.epi_bytes);
+  if (P.s.stages < 2 || smem > kUmmaSmemBudget || (P.s.epi_bytes & 255)) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(umma_gemm_kernel<BN, Epi, EG>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int tiles = P.s.batch * P.s.ksplit * P.s.mt * P.s.nt;
   const int grid = tiles < num_sms ? tiles : num_sms;
-  umma_gemm_kernel<BN, Epi><<<grid, 192, smem, st>>>(P);
+  umma_gemm_kernel<BN, Epi, EG><<<grid, 64 + 128 * EG, smem, st>>>(P);
   return cudaGetLastError();
 }
 
