@@ -468,9 +468,13 @@ int prop_launch(const Layout& L, const double* prep, double* work, int s, int nc
   P.s.ngroups = 2;
   P.s.kc = 4;
   // the propagator's epilogue (FP32 accumulator update, next operand pieces)
-  // outlasts its MMAs: two epilogue warpgroups when their staging fits
-  if (L.tune.prop_epi_groups != 1 &&
-      umma_pick_stages(BN, L.npc, L.npc, 2 * align256(umma_chunk_stage_bytes(BN))) >= 2)
+  // outlasts its MMAs: as many epilogue warpgroups (up to three) as their
+  // staging, two pipeline stages and one TMEM buffer per group allow
+  const size_t cs = align256(umma_chunk_stage_bytes(BN));
+  const int want = L.tune.prop_epi_groups ? L.tune.prop_epi_groups : 3;
+  if (want >= 3 && 3 * 2 * BN <= 512 && umma_pick_stages(BN, L.npc, L.npc, 3 * cs) >= 2)
+    return run<BN, 3>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
+  if (want >= 2 && umma_pick_stages(BN, L.npc, L.npc, 2 * cs) >= 2)
     return run<BN, 2>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
   return run<BN, 1>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
 }

@@ -12,10 +12,10 @@
 //               accumulators and commits stage/accumulator barriers
 //   warps 2..5  epilogue: tcgen05.ld rows of the finished accumulator (one TMEM
 //               lane per thread) and hand 32 columns at a time to the functor
-//   warps 6..9  (EG = 2) a second epilogue warpgroup.  The CTA's tiles then
-//               alternate between the groups, tile t in accumulator t & 1 for all
-//               its K chunks, so a long epilogue of one tile runs while the
-//               other group drains and processes the next tile
+//   warps 6..   (EG = 2, 3) more epilogue warpgroups.  The CTA's tiles then
+//               rotate over the groups, tile t in accumulator t % EG for all its
+//               K chunks, so a long epilogue of one tile runs while the other
+//               groups drain and process the next tiles
 // All waits are bounded; on timeout the CTA records an error and unwinds.
 #pragma once
 
@@ -74,10 +74,11 @@ struct UmmaParams {
   Epi epi;
 };
 
-// TMEM columns for two accumulator buffers of ngroups x bn fp32 columns
-__host__ __device__ constexpr int umma_tmem_cols(int bn, int ngroups = 1) {
+// TMEM columns for nbuf (two, or one per epilogue warpgroup) accumulator
+// buffers of ngroups x bn fp32 columns
+__host__ __device__ constexpr int umma_tmem_cols(int bn, int ngroups = 1, int nbuf = 2) {
   int c = 32;
-  while (c < 2 * ngroups * bn) c <<= 1;
+  while (c < nbuf * ngroups * bn) c <<= 1;
   return c;
 }
 
@@ -101,7 +102,8 @@ inline int umma_pick_stages(int bn, int npa, int npb, size_t extra) {
 template <int BN, class Epi, int EG>
 __global__ void __launch_bounds__(64 + 128 * EG, 1)
     umma_gemm_kernel(const __grid_constant__ UmmaParams<Epi> P) {
-  static_assert(EG == 1 || EG == 2, "one or two epilogue warpgroups");
+  static_assert(EG >= 1 && EG <= 3, "one to three epilogue warpgroups");
+  constexpr int NBUF = EG > 2 ? EG : 2;  // accumulator buffers
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M=128");
   static_assert(umma_tmem_cols(BN) <= 512, "two accumulators must fit in TMEM");
   extern __shared__ uint8_t smem_raw[];
@@ -113,11 +115,11 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * stage_bytes);
   uint64_t* empty = full + ST;
   uint64_t* accf = empty + ST;
-  uint64_t* acce = accf + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce + 2);
+  uint64_t* acce = accf + NBUF;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce + NBUF);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
   uint8_t* epi_smem = reinterpret_cast<uint8_t*>(full) + 256;  // epilogue scratch
-  const uint32_t kCols = umma_tmem_cols(BN, P.s.ngroups);
+  const uint32_t kCols = umma_tmem_cols(BN, P.s.ngroups, NBUF);
   const uint32_t acc_stride = (uint32_t)(P.s.ngroups * BN);  // columns per accumulator buffer
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -126,7 +128,7 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NBUF; ++b) {
       mbar_init(&accf[b], 1);
       mbar_init(&acce[b], 4);
     }
@@ -184,15 +186,15 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
       int stage = 0;
       uint32_t phase = 0;
       int it = 0, t = 0;
-      uint32_t uses[2] = {0u, 0u};  // EG = 2: chunks accumulated so far in each buffer
+      uint32_t uses[NBUF] = {};  // EG > 1: chunks accumulated so far in each buffer
       for (int tile = blockIdx.x; tile < tiles && !*abort_s; tile += gridDim.x, ++t) {
         const int k0 = ((tile / (S.nt * S.mt)) % S.ksplit) * S.kchunk;
         const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
         const int kc = S.kc > 0 ? S.kc : KB;
         bool ok = true;
         for (int c0 = 0; c0 < KB && ok; c0 += kc, ++it) {
-          const int buf = EG == 2 ? (t & 1) : (it & 1);
-          const uint32_t use = EG == 2 ? uses[buf]++ : (uint32_t)(it >> 1);
+          const int buf = EG > 1 ? (t % EG) : (it & 1);
+          const uint32_t use = EG > 1 ? uses[buf]++ : (uint32_t)(it >> 1);
           if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); ok = false; break; }
           tc_fence_after();
           const uint32_t dt = tbase + buf * acc_stride;
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
     uint32_t uses = 0;  // EG = 2: chunks drained from this group's buffer so far
     bool ok = true;
     for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++t) {
-      if (EG == 2 && (t & 1) != eg) continue;
+      if (EG > 1 && (t % EG) != eg) continue;
       const int nti = tile % S.nt, rest = tile / S.nt;
       const int mti = rest % S.mt, z = rest / S.mt;
       const int k0 = (z % S.ksplit) * S.kchunk;
@@ -240,8 +242,8 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
       const int kc = S.kc > 0 ? S.kc : KB;
       const int nch = (KB + kc - 1) / kc;
       for (int ch = 0; ch < nch; ++ch, ++it) {
-        const int buf = EG == 2 ? eg : (it & 1);
-        const uint32_t use = EG == 2 ? uses++ : (uint32_t)(it >> 1);
+        const int buf = EG > 1 ? eg : (it & 1);
+        const uint32_t use = EG > 1 ? uses++ : (uint32_t)(it >> 1);
         if (!mbar_wait_abortable(&accf[buf], use & 1, abort_s)) { fail(); ok = false; break; }
         tc_fence_after();
         const uint32_t taddr = tbase + ((uint32_t)(sub * 32) << 16) + buf * acc_stride;
@@ -290,7 +292,9 @@ int make_tmap_bf16(CUtensorMap* map, const void* base, long long K, long long ro
 template <int BN, int EG = 1, class Epi>
 cudaError_t launch_umma(const UmmaParams<Epi>& P, int num_sms, cudaStream_t st) {
   const size_t smem = umma_smem_bytes(BN, P.s.stages, P.s.npa, P.s.npb, size_t(EG) * P.s.epi_bytes);
-  if (P.s.stages < 2 || smem > kUmmaSmemBudget || (P.s.epi_bytes & 255)) return cudaErrorInvalidValue;
+  if (P.s.stages < 2 || smem > kUmmaSmemBudget || (P.s.epi_bytes & 255) ||
+      (EG > 2 ? EG : 2) * P.s.ngroups * BN > 512)
+    return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(umma_gemm_kernel<BN, Epi, EG>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

@@ -278,7 +278,7 @@ typedef struct afq_tuning {
   int32_t f64_exch_bn; /* FP64 exchange tile: 80, 120 or 160 (BM 120, 120, 128)           */
   int32_t max_stages;  /* cap on tcgen05 pipeline stages: 2..8                             */
   int32_t grid_cap;    /* CTAs of the persistent tensor-core kernels: 1..number of SMs     */
-  int32_t prop_epi_groups; /* epilogue warpgroups of the tensor-core propagator: 1 or 2    */
+  int32_t prop_epi_groups; /* epilogue warpgroups of the tensor-core propagator: 1 to 3    */
   int32_t reserved[8];
 } afq_tuning;
 
