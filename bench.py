@@ -140,6 +140,11 @@ def measured_peaks():
 # CUDA events; the driver's peaks file carries no FP64 figure).
 FP64_PEAK_TFLOPS = 35.47
 
+# DRAM bytes (read + written) per propagator launch, mean over the 7 launches
+# of one step, from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
+# bench workload (N=200, No=40, G=1000, 512 walkers, mixed).
+PROP_DRAM_BYTES_PER_LAUNCH = 256684727
+
 
 def main():
     args = parse()
@@ -284,7 +289,8 @@ def main():
     clk_path = os.path.join(tempfile.gettempdir(), f"afq_clocks_{rank}.csv")
     clk = clocks_start(clk_path)
     ms_total, (kern_ms, kern_n), launches, killed, (ham_data, wave, prop, pd) = timed_run(
-        args.precision, args.steps, args.warmup, "vhs", graph=not args.eager)
+        args.precision, args.steps, args.warmup, "vhs" if args.precision == "fp64" else "prop",
+        graph=not args.eager)
     clocks = clocks_stop(clk, clk_path, torch.cuda.current_device())
     value = world * W * S * args.steps / (ms_total / 1e3)
 
@@ -377,24 +383,47 @@ def main():
 
     # ---- roofline of the dominant kernel ------------------------------------
     N, G = sys_.norb, sys_.nchol
-    flops_per_launch = 4.0 * W * N * N * G  # C(2W x N^2) = Xt(2W x G) L(G x N^2)
     avg_ms = kern_ms / max(kern_n, 1)
-    achieved = flops_per_launch / (avg_ms / 1e3) / 1e12
     products = {"fp64": 1, "mixed": 3, "mixed_hi": 6}[args.precision]
     if args.precision == "fp64":
-        peak, peak_src = FP64_PEAK_TFLOPS, "measured (cuBLAS DGEMM on this pool)"
-        kname = "vhs_gemm_kernel (FP64 DMMA)"
+        # the FP64 VHS GEMM, tensor-bound: C(2W x N^2) = Xt(2W x G) L(G x N^2)
+        flops_per_launch = 4.0 * W * N * N * G
+        achieved = flops_per_launch / (avg_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "kernel": "vhs_gemm_kernel (FP64 DMMA)", "achieved": achieved,
+                "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s", "frac": achieved / FP64_PEAK_TFLOPS,
+                "peak_source": "measured (cuBLAS DGEMM on this pool)", "traffic": None,
+                "launches": kern_n, "avg_launch_ms": avg_ms, "flops_per_launch": flops_per_launch}
     else:
+        # the propagator GEMMs (7 launches per step, the largest share of a block), HBM-bound:
+        # algorithmic bytes of one step per spin sector s (nc = 2 No_s, npc bf16 pieces):
+        #   5 Taylor terms: VHS pieces W N 2N, iterate pieces W nc 2N, FP32 accumulator read and
+        #     written (W nc N), next iterate pieces W nc 2N (the last term: N columns)
+        #   2 one-body half-steps: (e^{-dt h/2} - I) pieces N N, walker/sum pieces W nc N,
+        #     accumulator read (+ written by the first), next pieces W nc 2N / walker W N nc
+        #     doubles out (the second)
+        npc = 2 if args.precision == "mixed" else 3
+        nsec = 1 if sys_.trial == "rhf" else 2
+        step_bytes = 0.0
+        for s_ in range(nsec):
+            nc = 2 * sys_.nelec[s_]
+            bf = 2.0 * npc
+            taylor = (W * N * 2 * N * bf + W * nc * 2 * N * bf + 2 * W * nc * N * 4.0)
+            step_bytes += 5 * taylor + 4 * W * nc * 2 * N * bf + W * nc * N * bf
+            step_bytes += 2 * (N * N * bf + W * nc * N * bf)           # the two half-steps' operands
+            step_bytes += 2 * W * nc * N * 4.0 + W * nc * 2 * N * bf   # first half-step: acc r/w, pieces
+            step_bytes += W * nc * N * 4.0 + W * N * nc * 8.0          # second: acc read, walker out
+        bytes_per_launch = step_bytes / 7.0
+        achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
         pk, src = measured_peaks()
-        peak, peak_src = pk["bf16_tflops"], src + " bf16 dense"
-        kname = f"umma_gemm_kernel<VhsEpiU> (tcgen05 BF16x{products})"
-    roof = {"bound": "tensor", "kernel": kname, "achieved": achieved, "peak": peak,
-            "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_src,
-            "traffic": None, "launches": kern_n, "avg_launch_ms": avg_ms,
-            "flops_per_launch": flops_per_launch,
-            "note": "achieved counts algorithmic flops 4*W*N^2*G per launch; the tensor pipe "
-                    f"executes {products}x that (split-operand products)",
-            "executed_tflops": achieved * products}
+        roof = {"bound": "hbm", "kernel": f"umma_gemm_kernel<PropEpiU> (tcgen05 BF16x{products}, "
+                                           "Taylor terms and one-body half-steps)",
+                "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / pk["hbm_gbs"], "peak_source": src + " HBM copy",
+                "traffic": PROP_DRAM_BYTES_PER_LAUNCH if W == 512 and args.config == CONFIG else None,
+                "launches": kern_n, "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
+                "note": "average over the 7 launches of a step; traffic = ncu dram bytes read+written "
+                        "per launch on this workload (the VHS pieces, 164 MB, are read by each of the "
+                        "5 Taylor launches)"}
 
     cpu = None
     if not args.no_cpu:
