@@ -114,11 +114,14 @@ __device__ void qr_inplace(double2* A, int lda, int N, int no, double2* tau, dou
       __syncthreads();
       // A[p][j] -= conj(tau) v_p w_j     (H^H applied from the left)
       const double2 ct = cconj(tk);
-      const int rows = N - k;
-      for (int e = tid; e < rows * nj; e += T) {
-        const int p = k + e / nj, j = e - (e / nj) * nj;
-        const double2 vp = A[p * lda + k];
-        A[p * lda + k + 1 + j] = csub(A[p * lda + k + 1 + j], cmul(ct, cmul(vp, wv[j])));
+      // thread -> (row offset, column) once per column; rows advance by T / nj
+      const int pstep = T / nj, j = tid % nj;
+      if (tid < pstep * nj) {
+        const double2 cw = cmul(ct, wv[j]);
+        for (int p = k + tid / nj; p < N; p += pstep) {
+          const double2 vp = A[p * lda + k];
+          A[p * lda + k + 1 + j] = csub(A[p * lda + k + 1 + j], cmul(vp, cw));
+        }
       }
       __syncthreads();
     }
@@ -146,11 +149,13 @@ __device__ void qr_inplace(double2* A, int lda, int N, int no, double2* tau, dou
         wv[j] = acc;
       }
       __syncthreads();
-      const int rows = N - i;
-      for (int e = tid; e < rows * nj; e += T) {
-        const int p = i + e / nj, j = e - (e / nj) * nj;
-        const double2 vp = A[p * lda + i];
-        A[p * lda + i + 1 + j] = csub(A[p * lda + i + 1 + j], cmul(ti, cmul(vp, wv[j])));
+      const int pstep = T / nj, j = tid % nj;
+      if (tid < pstep * nj) {
+        const double2 cw = cmul(ti, wv[j]);
+        for (int p = i + tid / nj; p < N; p += pstep) {
+          const double2 vp = A[p * lda + i];
+          A[p * lda + i + 1 + j] = csub(A[p * lda + i + 1 + j], cmul(vp, cw));
+        }
       }
       __syncthreads();
     }
