@@ -61,13 +61,17 @@ GreenArgs green_args_mo(const Layout& L, const double* const mo[2], double* work
   a.npc = L.npc;
   for (int i = 0; i < 3; ++i) a.gplb[i] = nullptr;
   a.ldgb = L.Kb;
+  a.sbuf = nullptr;
+  a.sstride = (long long)L.nomax * L.nomax;
   return a;
 }
 
 GreenArgs green_args(const Layout& L, const double* prep, double* work,
                      const double* const walkers[2]) {
   const double* mo[2] = {prep + L.p_mo[0], prep + L.p_mo[1]};
-  return green_args_mo(L, mo, work, walkers);
+  GreenArgs a = green_args_mo(L, mo, work, walkers);
+  a.sbuf = work + L.w_s;  // the full workspace: S goes through the warp-level inverse
+  return a;
 }
 
 int check_small(const afq_dims* d, Layout& L, void* work, size_t work_bytes) {

@@ -22,90 +22,17 @@ namespace {
 constexpr int kGreenThreads = 256;
 constexpr int kRowChunk = 32;
 
-__global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
-  extern __shared__ double2 sm[];
-  const int w = blockIdx.x, sct = blockIdx.y;
-  const GreenSector& S_ = a.sec[sct];
-  const int N = a.N, no = S_.no, tid = threadIdx.x;
+// Gauss-Jordan inverse with partial pivoting of the No x No complex S in
+// shared memory, in place, by the whole CTA (kGreenThreads threads); returns
+// det S in thread 0.
+__device__ double2 gauss_jordan_cta(double2* S, double2* colk, int* perm, double2* ipk_s, int no) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr int T = kGreenThreads;
-
-  double2* S = sm;                          // no*no
-  double2* colk = S + no * no;              // 64
-  double2* stage = colk + 64;               // kRowChunk*no   (walker rows, C^T W phase)
-  double* moc = reinterpret_cast<double*>(stage + kRowChunk * no);  // kRowChunk*no
-  double2* tstage = reinterpret_cast<double2*>(moc + kRowChunk * no);  // kRowChunk*(no+1)
-  const int ts = no + 1;  // padded row stride of tstage (conflict-free column reads)
-  __shared__ double red[2 * (T / 32)];
-  __shared__ int perm[64];
-
-  const double2* Wg =
-      reinterpret_cast<const double2*>(S_.walk) + (long long)w * N * no;
-
-  // ---- S = C^T W on the FP64 tensor cores ----------------------------------
-  // As real matrices: S (No x 2No, (re, im) interleaved) = C^T (No x N) times
-  // W (N x 2No, the complex walker viewed as doubles).  mma.m8n8k4 tiles: warp
-  // w owns column tiles w and w + 8 and every row tile, so each B fragment is
-  // loaded once per k-step.  Rows of W and C are staged 32 at a time.
-  const int warp = tid >> 5, lane = tid & 31;
-  const int nc2 = 2 * no;
-  const int mtiles = (no + 7) >> 3, ntiles = (nc2 + 7) >> 3;  // <= 8, <= 16
-  const double* stageD = reinterpret_cast<const double*>(stage);
-  double sacc[2][8][2];
-#pragma unroll
-  for (int sl = 0; sl < 2; ++sl)
-#pragma unroll
-    for (int mi = 0; mi < 8; ++mi) sacc[sl][mi][0] = sacc[sl][mi][1] = 0.0;
-  for (int p0 = 0; p0 < N; p0 += kRowChunk) {
-    const int rows = min(kRowChunk, N - p0);
-    for (int e = tid; e < rows * no; e += T) {
-      stage[e] = Wg[(long long)p0 * no + e];
-      moc[e] = S_.mo[(long long)p0 * no + e];
-    }
-    __syncthreads();
-    for (int kk = 0; kk < rows; kk += 4) {
-      const int kr = kk + (lane & 3);
-      const bool kin = kr < rows;
-      double afr[8];
-#pragma unroll
-      for (int mi = 0; mi < 8; ++mi) {
-        const int m = mi * 8 + (lane >> 2);
-        afr[mi] = (mi < mtiles && kin && m < no) ? moc[kr * no + m] : 0.0;
-      }
-#pragma unroll
-      for (int sl = 0; sl < 2; ++sl) {
-        const int ni = warp + sl * 8;
-        if (ni < ntiles) {  // warp-uniform
-          const int n = ni * 8 + (lane >> 2);
-          const double b = (kin && n < nc2) ? stageD[kr * nc2 + n] : 0.0;
-#pragma unroll
-          for (int mi = 0; mi < 8; ++mi)
-            if (mi < mtiles) dmma_8x8x4(sacc[sl][mi][0], sacc[sl][mi][1], afr[mi], b);
-        }
-      }
-    }
-    __syncthreads();
-  }
   const int npairs = no * no;
-#pragma unroll
-  for (int sl = 0; sl < 2; ++sl) {
-    const int ni = warp + sl * 8;
-    if (ni < ntiles) {
-#pragma unroll
-      for (int mi = 0; mi < 8; ++mi) {
-        const int i = mi * 8 + (lane >> 2), j = ni * 4 + (lane & 3);
-        if (mi < mtiles && i < no && j < no)
-          S[i * no + j] = make_double2(sacc[sl][mi][0], sacc[sl][mi][1]);
-      }
-    }
-  }
-  __syncthreads();
-
-  // ---- Gauss-Jordan inverse with partial pivoting, det ----------------------
   // Each elimination step: warp 0 alone finds the pivot (first max of
   // |re|+|im| in column k, as LAPACK izamax), swaps it into row k, keeps
   // column k and scales row k by 1/p (= conj(p)/|p|^2); then every thread
   // updates its fixed elements.  Two block barriers per step.
-  __shared__ double2 ipk_s;
   int my_i[16], my_j[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) {
@@ -145,13 +72,13 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
       for (int j = lane; j < no; j += 32) S[k * no + j] = (j == k) ? ipk : cmul(S[k * no + j], ipk);
       if (lane == 0) {
         perm[k] = pv;
-        ipk_s = ipk;
+        *ipk_s = ipk;
         det = cmul(det, pk);
         if (pv != k) det = make_double2(-det.x, -det.y);
       }
     }
     __syncthreads();
-    const double2 ipk = ipk_s;
+    const double2 ipk = *ipk_s;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
       const int i = my_i[q], j = my_j[q];
@@ -177,10 +104,111 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
       }
     }
   __syncthreads();
+  return det;
+}
+
+// mode 0: the whole computation; 1: S = C^T W only, into a.sbuf; 2: Theta
+// and its outputs from S^-1 in a.sbuf (the inverse and det by gj_kernel)
+__global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int mode) {
+  extern __shared__ double2 sm[];
+  const int w = blockIdx.x, sct = blockIdx.y;
+  const GreenSector& S_ = a.sec[sct];
+  const int N = a.N, no = S_.no, tid = threadIdx.x;
+  constexpr int T = kGreenThreads;
+
+  double2* S = sm;                          // no*no
+  double2* colk = S + no * no;              // 64
+  double2* stage = colk + 64;               // kRowChunk*no   (walker rows, C^T W phase)
+  double* moc = reinterpret_cast<double*>(stage + kRowChunk * no);  // kRowChunk*no
+  double2* tstage = reinterpret_cast<double2*>(moc + kRowChunk * no);  // kRowChunk*(no+1)
+  const int ts = no + 1;  // padded row stride of tstage (conflict-free column reads)
+  __shared__ double red[2 * (T / 32)];
+  __shared__ int perm[64];
+
+  const double2* Wg =
+      reinterpret_cast<const double2*>(S_.walk) + (long long)w * N * no;
+
+  // ---- S = C^T W on the FP64 tensor cores ----------------------------------
+  // As real matrices: S (No x 2No, (re, im) interleaved) = C^T (No x N) times
+  // W (N x 2No, the complex walker viewed as doubles).  mma.m8n8k4 tiles: warp
+  // w owns column tiles w and w + 8 and every row tile, so each B fragment is
+  // loaded once per k-step.  Rows of W and C are staged 32 at a time.
+  const int warp = tid >> 5, lane = tid & 31;
+  const int nc2 = 2 * no;
+  const int mtiles = (no + 7) >> 3, ntiles = (nc2 + 7) >> 3;  // <= 8, <= 16
+  const double* stageD = reinterpret_cast<const double*>(stage);
+  double2* sg = a.sbuf ? reinterpret_cast<double2*>(a.sbuf) + ((long long)sct * a.W + w) * a.sstride
+                       : nullptr;
+  const int npairs = no * no;
+  if (mode != 2) {
+  double sacc[2][8][2];
+#pragma unroll
+  for (int sl = 0; sl < 2; ++sl)
+#pragma unroll
+    for (int mi = 0; mi < 8; ++mi) sacc[sl][mi][0] = sacc[sl][mi][1] = 0.0;
+  for (int p0 = 0; p0 < N; p0 += kRowChunk) {
+    const int rows = min(kRowChunk, N - p0);
+    for (int e = tid; e < rows * no; e += T) {
+      stage[e] = Wg[(long long)p0 * no + e];
+      moc[e] = S_.mo[(long long)p0 * no + e];
+    }
+    __syncthreads();
+    for (int kk = 0; kk < rows; kk += 4) {
+      const int kr = kk + (lane & 3);
+      const bool kin = kr < rows;
+      double afr[8];
+#pragma unroll
+      for (int mi = 0; mi < 8; ++mi) {
+        const int m = mi * 8 + (lane >> 2);
+        afr[mi] = (mi < mtiles && kin && m < no) ? moc[kr * no + m] : 0.0;
+      }
+#pragma unroll
+      for (int sl = 0; sl < 2; ++sl) {
+        const int ni = warp + sl * 8;
+        if (ni < ntiles) {  // warp-uniform
+          const int n = ni * 8 + (lane >> 2);
+          const double b = (kin && n < nc2) ? stageD[kr * nc2 + n] : 0.0;
+#pragma unroll
+          for (int mi = 0; mi < 8; ++mi)
+            if (mi < mtiles) dmma_8x8x4(sacc[sl][mi][0], sacc[sl][mi][1], afr[mi], b);
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int sl = 0; sl < 2; ++sl) {
+    const int ni = warp + sl * 8;
+    if (ni < ntiles) {
+#pragma unroll
+      for (int mi = 0; mi < 8; ++mi) {
+        const int i = mi * 8 + (lane >> 2), j = ni * 4 + (lane & 3);
+        if (mi < mtiles && i < no && j < no) {
+          const double2 v = make_double2(sacc[sl][mi][0], sacc[sl][mi][1]);
+          if (mode == 1)
+            sg[i * no + j] = v;
+          else
+            S[i * no + j] = v;
+        }
+      }
+    }
+  }
+  if (mode == 1) return;
+  __syncthreads();
+  }  // mode != 2
+  if (mode == 2) {  // S^-1 from gj_kernel
+    for (int e = tid; e < npairs; e += T) S[e] = sg[e];
+    __syncthreads();
+  } else {
+
+  // ---- Gauss-Jordan inverse with partial pivoting, det ----------------------
+  __shared__ double2 ipk_s;
+  const double2 det = gauss_jordan_cta(S, colk, perm, &ipk_s, no);
   if (tid == 0 && a.wscal) {
     a.wscal[(long long)w * 16 + 4 + 2 * sct] = det.x;
     a.wscal[(long long)w * 16 + 5 + 2 * sct] = det.y;
   }
+  }  // mode 0: inverse in this CTA
 
   const bool need_theta = S_.theta || S_.gout || a.gpl || S_.rh1 || a.gplb[0] || S_.gtb[0];
   if (!need_theta) return;
@@ -287,6 +315,31 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a) {
   }
 }
 
+// Gauss-Jordan inverse and det of S = C^T W held in sbuf, one CTA per
+// (walker, sector), in place (the arithmetic of the whole-computation mode).
+// Only S, its pivot column and the permutation live in shared memory, so
+// several CTAs share an SM and hide each other's barrier latency.
+__global__ void __launch_bounds__(kGreenThreads, 4)
+    gj_kernel(int W, int no0, int no1, double* sbuf, long long sstride, double* wscal) {
+  extern __shared__ double2 gsm[];
+  const int w = blockIdx.x, sct = blockIdx.y;
+  const int no = sct ? no1 : no0;
+  double2* S = gsm;
+  double2* colk = S + sstride;
+  __shared__ int perm[64];
+  __shared__ double2 ipk_s;
+  double2* g = reinterpret_cast<double2*>(sbuf) + ((long long)sct * W + w) * sstride;
+  const int nn = no * no;
+  for (int e = threadIdx.x; e < nn; e += kGreenThreads) S[e] = g[e];
+  __syncthreads();
+  const double2 det = gauss_jordan_cta(S, colk, perm, &ipk_s, no);
+  for (int e = threadIdx.x; e < nn; e += kGreenThreads) g[e] = S[e];
+  if (threadIdx.x == 0 && wscal) {
+    wscal[(long long)w * 16 + 4 + 2 * sct] = det.x;
+    wscal[(long long)w * 16 + 5 + 2 * sct] = det.y;
+  }
+}
+
 __global__ void ovlp_combine_kernel(int W, int ns, int mult, const double* wscal, double* out,
                                     int out_stride) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -316,7 +369,24 @@ cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   dim3 grid(a.W, a.ns);
   ProfScope ps(K_GREEN, st);
-  green_kernel<<<grid, kGreenThreads, smem, st>>>(a);
+  bool need_theta = a.gpl || a.gplb[0];
+  for (int s = 0; s < a.ns; ++s)
+    need_theta = need_theta || a.sec[s].theta || a.sec[s].gout || a.sec[s].rh1 || a.sec[s].gtb[0];
+  if (!a.sbuf || !need_theta) {  // one kernel: S, its inverse and det, Theta and outputs
+    green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 0);
+    return cudaGetLastError();
+  }
+  // S into a.sbuf; warp-level inverse and det; Theta and its outputs
+  green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 1);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const size_t gsmem = (size_t(a.sstride) + 64) * sizeof(double2);
+  if ((e = cudaFuncSetAttribute(gj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem)) !=
+      cudaSuccess)
+    return e;
+  gj_kernel<<<grid, kGreenThreads, gsmem, st>>>(a.W, a.sec[0].no, a.ns > 1 ? a.sec[1].no : 0,
+                                                a.sbuf, a.sstride, a.wscal);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 2);
   return cudaGetLastError();
 }
 

@@ -109,7 +109,7 @@ struct Layout {
   long long p_mo[2], p_rh1[2], p_rc[2], p_rccat, p_chol, p_exph1[2], p_mf, p_scal, prepared;
   // workspace offsets (doubles)
   long long w_gpl, w_theta[2], w_fbpart, w_xt, w_wscal, w_vhs, w_y, w_acc, w_ta, w_tb;
-  long long w_c[2], w_exc[2], w_orb, w_cum, w_idx, w_misc, work;
+  long long w_c[2], w_exc[2], w_orb, w_s, w_cum, w_idx, w_misc, work;
 };
 
 inline ExchTile choose_exch_tile(int no, int G, int W) {
@@ -302,6 +302,8 @@ inline int make_layout(const afq_dims* d, Layout& L, const afq_tuning* record = 
   for (int s = 0; s < L.ns; ++s) L.w_exc[s] = take((long long)L.ex[s].mt * W * 2);
   // LNO orbital-energy partials per FP64 exchange row tile (restricted walkers)
   L.w_orb = take((long long)((L.G + L.ex[0].gpt - 1) / L.ex[0].gpt) * W * 2);
+  // S and S^-1 of the Green's function per (sector, walker), No_max^2 complex each
+  L.w_s = take((long long)L.ns * W * L.nomax * L.nomax * 2);
   L.work = o;
   return AFQ_OK;
 }

@@ -29,6 +29,8 @@ struct GreenArgs {
   int npc;              // bf16 pieces for the *b outputs
   bf16* gplb[3];        // force-bias operand pieces (2W, ldgb) or nullptr
   long long ldgb;
+  double* sbuf;         // (ns, W, sstride) complex scratch for S and S^-1, or nullptr (one kernel)
+  long long sstride;    // complex elements per (sector, walker): No_max^2
 };
 cudaError_t launch_green(const GreenArgs& a, cudaStream_t st);
 // overlaps from per-sector determinants in wscal: out[w] = det0^mult (or det0*det1)
