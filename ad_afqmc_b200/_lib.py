@@ -124,6 +124,8 @@ _SIGS = {
     "afq_stochastic_reconfiguration_dev": ([C.POINTER(afq_dims), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p * 2, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "afq_normal_fields_dev": ([C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
     "afq_uniform_dev": ([C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p], C.c_int),
+    "afq_apply_trotprop": ([C.POINTER(afq_dims), C.c_void_p, C.c_void_p * 2, C.c_void_p, C.c_void_p, C.c_size_t,
+                            C.c_void_p], C.c_int),
     "afq_calc_orbenergy": ([C.POINTER(afq_dims), C.c_void_p, C.c_void_p * 2, C.c_void_p, C.c_int32, C.c_void_p,
                             C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
     "afq_comb_indices_ranks": ([C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p, C.c_void_p,

@@ -350,6 +350,27 @@ int afq_propagate_constrained(const afq_dims* d, const void* prepared, afq_state
   return AFQ_OK;
 }
 
+int afq_apply_trotprop(const afq_dims* d, const void* prepared, double* const walkers[2],
+                       const double* fields, void* work, size_t work_bytes, void* stream) {
+  Layout L;
+  int rc = check_common(d, L, prepared, work, work_bytes);
+  if (rc != AFQ_OK) return rc;
+  if (!walkers || !fields) return AFQ_ERR_NULL;
+  const double* const wc[2] = {walkers[0], walkers[1]};
+  if ((rc = check_walkers(L, wc)) != AFQ_OK) return rc;
+  const double* P = static_cast<const double*>(prepared);
+  double* Wk = static_cast<double*>(work);
+  cudaStream_t st = as_stream(stream);
+  AFQ_TRY(launch_free_fields(L, Wk, fields, d->dt, st));
+  if (L.mixed) {
+    if ((rc = mixed_vhs_gemm(L, P, Wk, st)) != AFQ_OK) return rc;
+    return mixed_propagate_walkers(L, P, Wk, walkers, d->n_exp_terms, st);
+  }
+  AFQ_TRY(launch_vhs_gemm(L, P, Wk, st));
+  AFQ_TRY(launch_propagate_walkers(L, P, Wk, walkers, d->n_exp_terms, st));
+  return AFQ_OK;
+}
+
 int afq_orthonormalize(const afq_dims* d, double* const walkers[2], double* norms, void* work,
                        size_t work_bytes, void* stream) {
   Layout L;

@@ -470,6 +470,35 @@ cudaError_t launch_prep(const Layout& L, const double* prep, double* work, const
   return cudaGetLastError();
 }
 
+// Free propagation (propagation.py:338-376): VHS = i sqrt(dt) x L from the raw
+// fields x, rows (w, 0) = Re = 0 and (w, 1) = Im = sqrt(dt) x of the VHS operand
+__global__ void __launch_bounds__(256) free_fields_kernel(int G, long long Gpad, const double* fields,
+                                                          double sdt, double* xt, int npc, bf16* xb0,
+                                                          bf16* xb1, bf16* xb2, long long ldxb) {
+  bf16* const xb[3] = {xb0, xb1, xb2};
+  const int w = blockIdx.x;
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    const double x = fields[(long long)w * G + g];
+    if (xb0) {
+      put_pieces(0.0, npc, xb, (2LL * w) * ldxb + g);
+      put_pieces(sdt * x, npc, xb, (2LL * w + 1) * ldxb + g);
+    } else {
+      xt[(2LL * w) * Gpad + g] = 0.0;
+      xt[(2LL * w + 1) * Gpad + g] = sdt * x;
+    }
+  }
+}
+
+cudaError_t launch_free_fields(const Layout& L, double* work, const double* fields, double dt,
+                               cudaStream_t st) {
+  ProfScope ps(K_PREP, st);
+  bf16* xb[3] = {nullptr, nullptr, nullptr};
+  if (L.mixed) piece_ptrs(work, L.v_xt, L.v_xt_ps, L.npc, xb);
+  free_fields_kernel<<<L.W, 256, 0, st>>>(L.G, L.Gpad, fields, sqrt(dt), work + L.w_xt, L.npc, xb[0],
+                                          xb[1], xb[2], L.Gb);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_vhs_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {
   using Cfg = CfgBig;
   const int M = 2 * L.W, NN = L.N * L.N, K = L.G;

@@ -42,6 +42,8 @@ cudaError_t launch_fb_gemm(const Layout& L, const double* prepared, double* work
                            cudaStream_t st);
 cudaError_t launch_prep(const Layout& L, const double* prepared, double* work,
                         const double* fields, double dt, double* fb_out, cudaStream_t st);
+cudaError_t launch_free_fields(const Layout& L, double* work, const double* fields, double dt,
+                               cudaStream_t st);
 cudaError_t launch_vhs_gemm(const Layout& L, const double* prepared, double* work,
                             cudaStream_t st);
 cudaError_t launch_propagate_walkers(const Layout& L, const double* prepared, double* work,

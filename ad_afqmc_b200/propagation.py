@@ -195,6 +195,45 @@ class propagator_afqmc(propagator):
         note_state(prop_data, st, eng)
         return prop_data
 
+    def propagate_free(self, trial, ham_data: dict, prop_data: dict, fields, wave_data: dict) -> dict:
+        """Free propagation, propagation.py:338-376: the Trotterized propagator
+        with the raw fields (afq_apply_trotprop), the mean-field constants
+        exp(-sqrt(dt) x.mf_shifts_fp) exp(dt h0_prop_fp), orthogonalization
+        with the norms into the weights, a local comb and the new overlaps."""
+        if self.walker_type not in ("restricted", "unrestricted"):
+            raise AssertionError("Free propagation is only implemented for restricted and unrestricted walkers.")
+        eng = self.engine(ham_data, trial, wave_data)
+        if not eng.has_prop:
+            raise _lib.AfqError("propagation intermediates missing: call build_propagation_intermediates")
+        f = to_dev(fields, torch.float64)
+        if f.shape != (self.n_walkers, int(ham_data["chol"].shape[0])):
+            raise ValueError(f"fields must be (n_walkers, nchol), got {tuple(f.shape)}")
+        sdt = self.dt ** 0.5
+        mf = to_dev(ham_data["mf_shifts_fp"], torch.complex128)
+        h0p = to_dev(torch.as_tensor(ham_data["h0_prop_fp"]), torch.complex128)
+        fc = f.to(torch.complex128)
+        if self.walker_type == "unrestricted":
+            constants = torch.exp(-sdt * (mf @ fc.T)) * torch.exp(self.dt * h0p).reshape(-1, 1)
+        else:
+            constants = torch.exp(-sdt * (fc @ mf)) * torch.exp(self.dt * h0p)
+        walkers = prop_data["walkers"]
+        data = [t.clone() for t in (walkers.data if isinstance(walkers, UHFWalkers) else [walkers.data])]
+        ptrs = _lib.pair(data[0].data_ptr(), data[-1].data_ptr() if len(data) > 1 else None)
+        p, w, wb = eng.handle
+        _lib.check(_lib.lib().afq_apply_trotprop(C.byref(eng.dims), p, ptrs, f.data_ptr(), w, wb,
+                                                 _lib.stream_handle()), "afq_apply_trotprop")
+        walkers = UHFWalkers(data) if isinstance(walkers, UHFWalkers) else RHFWalkers(data[0])
+        walkers = walkers.multiply_constants(constants)
+        walkers, norms = walkers.orthogonalize()
+        prop_data["weights"] = prop_data["weights"] * torch.real(norms)
+        zeta = prop_data["key"].uniform() if getattr(self, "_zeta_source", None) is None else \
+            float(self._zeta_source.uniform())
+        prop_data["walkers"], prop_data["weights"] = walkers.stochastic_reconfiguration_local(
+            prop_data["weights"], zeta)
+        prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+        prop_data.pop("_afq_green_of", None)
+        return prop_data
+
     def _build_propagation_intermediates(self, ham_data: dict, trial, wave_data: dict) -> dict:
         """mf_shifts, h0_prop, *_fp, exp_h1 (propagation.py:378-438), on the device."""
         n = trial.norb

@@ -91,6 +91,39 @@ class sampler:
         prop_data["block_energies"] = out
         return torch.sum(be * bw) / torch.sum(bw), prop_data
 
+    def propagate_free(self, ham, ham_data: dict, prop, prop_data: dict, trial, wave_data: dict):
+        """Free projection, sampling.py:367-384 over _block_scan_free (:96-144):
+        n_blocks blocks of n_prop_steps free steps.  Returns (ov, abs_ov,
+        prop_data_tr, block_energy, block_weight, key): per block the sum of
+        overlaps and of their moduli, a copy of the walker state, the
+        overlap-weighted energy (clamped against ene0, complex) and its weight."""
+        prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+        nchol = int(ham_data["chol"].shape[0])
+        ene0 = float(ham_data.get("ene0", 0.0))
+        lim = (2.0 / prop.dt) ** 0.5
+        prop._zeta_source = self.field_source
+        ov, aov, be, bw, states = [], [], [], [], []
+        try:
+            for _ in range(self.n_blocks):
+                fields = self._fields(prop, prop_data, nchol)
+                for s in range(self.n_prop_steps):
+                    prop_data = prop.propagate_free(trial, ham_data, prop_data, fields[s], wave_data)
+                e = trial.calc_energy(prop_data["walkers"], ham_data, wave_data)
+                e = torch.where(torch.abs(e - ene0) > lim, torch.full_like(e, ene0), e)
+                o = prop_data["overlaps"]
+                ow = o * prop_data["weights"]
+                be.append(torch.sum(e * ow) / torch.sum(ow))
+                bw.append(torch.sum(ow))
+                ov.append(torch.sum(o))
+                aov.append(torch.sum(torch.abs(o)))
+                w = prop_data["walkers"]
+                states.append({"walkers": [t.clone() for t in w.data] if isinstance(w.data, list) else w.data.clone(),
+                               "weights": prop_data["weights"].clone(), "overlaps": o.clone()})
+        finally:
+            prop._zeta_source = None
+        return (torch.stack(ov), torch.stack(aov), states, torch.stack(be), torch.stack(bw),
+                prop_data["key"])
+
     def __hash__(self) -> int:
         return hash((self.n_prop_steps, self.n_ene_blocks, self.n_sr_blocks, self.n_blocks))
 

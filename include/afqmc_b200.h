@@ -178,6 +178,14 @@ int afq_propagate_constrained(const afq_dims* d, const void* prepared, afq_state
 int afq_orthonormalize(const afq_dims* d, double* const walkers[2], double* norms, void* work,
                        size_t work_bytes, void* stream);
 
+/* walkers <- e^{-dt h/2} Taylor(e^{VHS}) e^{-dt h/2} walkers with VHS = i sqrt(dt)
+ * sum_g x[w,g] L_g from the raw fields (W, G) float64, in place: the
+ * propagator of free projection, propagator._apply_trotprop
+ * (propagation.py:178-229) as called by propagate_free (:338-376).  Needs the
+ * propagation intermediates (exp_h1, mf_shifts) in afq_prepare. */
+int afq_apply_trotprop(const afq_dims* d, const void* prepared, double* const walkers[2],
+                       const double* fields, void* work, size_t work_bytes, void* stream);
+
 /* Comb resampling: indices (W,) int32 and new weights from weights and zeta;
  * the walkers are gathered from walkers_in into walkers_out (distinct buffers).
  * mode AFQ_SR_LOCAL follows sr.py:24-48, AFQ_SR_GLOBAL the single-rank

@@ -299,6 +299,15 @@ def qr_unrestricted(walkers: List[np.ndarray]):
     return [q0, q1], np.array([np.abs(n0), np.abs(n1)])
 
 
+def orthogonalize(walkers):
+    """walkers.py:159-162 (norms**2) and :264-267 (|norm_up| |norm_dn|)."""
+    if isinstance(walkers, list):
+        q, n = qr_unrestricted(walkers)
+        return q, n[0] * n[1]
+    q, n = qr_restricted(walkers)
+    return q, n ** 2
+
+
 def orthonormalize(walkers):
     """walkers.py:155-157 (RHFWalkers) and :260-262 (UHFWalkers)."""
     if isinstance(walkers, list):
@@ -459,6 +468,27 @@ class Propagator:
         return np.array([self.apply_trotprop_single_det_vhs(w, v, ham_data["exp_h1"])
                          for w, v in zip(walkers, vhs)])
 
+    def propagate_free(self, trial, ham_data, prop_data, fields, wave_data, zeta):
+        """propagation.py:338-376 (zeta injected in place of the key split)."""
+        sdt = np.sqrt(self.dt)
+        if self.walker_type == "unrestricted":
+            shift = np.einsum("wg,sg->sw", fields, ham_data["mf_shifts_fp"])
+            const = np.exp(-sdt * shift) * np.exp(self.dt * np.asarray(ham_data["h0_prop_fp"])).reshape(-1, 1)
+        else:
+            shift = fields @ ham_data["mf_shifts_fp"]
+            const = np.exp(-sdt * shift) * np.exp(self.dt * ham_data["h0_prop_fp"])
+        w = self.apply_trotprop(prop_data["walkers"], fields, ham_data, trial.norb)
+        if isinstance(w, list):
+            w = [w[0] * const[0].reshape(-1, 1, 1), w[1] * const[1].reshape(-1, 1, 1)]
+        else:
+            w = w * const.reshape(-1, 1, 1)
+        w, norms = orthogonalize(w)
+        prop_data["weights"] = prop_data["weights"] * norms.real
+        prop_data["walkers"], prop_data["weights"] = stochastic_reconfiguration(
+            w, prop_data["weights"], zeta)
+        prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+        return prop_data
+
     def propagate_constrained(self, trial, ham_data, prop_data, fields, wave_data):
         """propagation.py:274-336."""
         sdt = np.sqrt(self.dt)
@@ -576,6 +606,29 @@ class Sampler:
         be, bw = np.array(be), np.array(bw)
         prop_data["n_killed_walkers"] /= self.n_sr_blocks * self.n_ene_blocks * prop.n_walkers
         return np.sum(be * bw) / np.sum(bw), prop_data
+
+
+def sampler_propagate_free(sampler, prop, trial, ham_data, prop_data, wave_data, rnd):
+    """sampling.py:96-144 (_block_scan_free) over sampling.py:367-384
+    (propagate_free): n_blocks blocks of n_prop_steps free steps; per block the
+    overlap-weighted energy (clamped against ene0), its weight, sum of overlaps
+    and of their moduli.  Returns (ov, abs_ov, block_energy, block_weight)."""
+    prop_data["overlaps"] = trial.calc_overlap(prop_data["walkers"], wave_data)
+    n_chol = np.asarray(ham_data["chol"]).shape[0]
+    ov, aov, be, bw = [], [], [], []
+    for _ in range(sampler.n_blocks):
+        fields = rnd.fields(sampler.n_prop_steps, prop.n_walkers, n_chol)
+        for s in range(sampler.n_prop_steps):
+            prop_data = prop.propagate_free(trial, ham_data, prop_data, fields[s], wave_data, rnd.uniform())
+        e = trial.calc_energy(prop_data["walkers"], ham_data, wave_data)
+        ene0 = ham_data.get("ene0", 0.0)
+        e = np.where(np.abs(e - ene0) > np.sqrt(2.0 / prop.dt), ene0, e)
+        o, w = prop_data["overlaps"], prop_data["weights"]
+        be.append(np.sum(e * o * w) / np.sum(o * w))
+        bw.append(np.sum(o * w))
+        ov.append(np.sum(o))
+        aov.append(np.sum(np.abs(o)))
+    return np.array(ov), np.array(aov), np.array(be), np.array(bw)
 
 
 class SamplerLNO(Sampler):
