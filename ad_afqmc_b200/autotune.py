@@ -18,6 +18,10 @@ Knobs (0 = the built-in rule):
   f64_exch_bn       FP64 exchange tile (FP64 path, or spins whose tensor-core
                     tile does not fit shared memory)
   max_stages        cap on the tcgen05 pipeline depth
+  prop_order        tile order of the tensor-core propagator launches: 0
+                    alternates the direction over the walkers from one launch
+                    to the next (each starts where the previous one ended, on
+                    data still in L2), 1 always runs forward
   grid_cap          CTAs of the persistent kernels (a batch-level knob: a
                     solve alone never gains from fewer CTAs, but overlapping
                     fragments can; ``tune_batch`` sweeps it for a whole batch)
@@ -40,7 +44,7 @@ import torch
 from . import _lib
 from .walkers import UHFWalkers
 
-_KNOB_ORDER = ("vhs_bn", "fb_bn", "fb_splitk", "exch_bn", "f64_exch_bn", "max_stages")
+_KNOB_ORDER = ("vhs_bn", "fb_bn", "fb_splitk", "exch_bn", "f64_exch_bn", "max_stages", "prop_order")
 
 
 def shape_key(d: _lib.afq_dims) -> str:
@@ -53,7 +57,7 @@ def candidates(d: _lib.afq_dims) -> Dict[str, List[int]]:
     out: Dict[str, List[int]] = {"fb_splitk": [1, 2, 4, 8], "f64_exch_bn": [80, 120, 160]}
     if mixed:
         out.update({"vhs_bn": [64, 128], "fb_bn": [64, 128], "exch_bn": [32, 64, 80, 96, 128],
-                    "max_stages": [2, 3, 4]})
+                    "max_stages": [2, 3, 4], "prop_order": [1]})
     return out
 
 

@@ -445,7 +445,7 @@ template <int BN>
 int prop_launch(const Layout& L, const double* prep, double* work, int s, int nc, int mode,
                 float scale, bf16* const a[3], long long aK, long long ald, long long abs,
                 int a_batched, bf16* const bsrc[3], bf16* const bdst[3], double* wout,
-                cudaStream_t st) {
+                int seq, cudaStream_t st) {
   UmmaParams<PropEpiU> P{};
   const int N = L.N;
   const long long btbs = 2LL * L.nomax * L.Kv;
@@ -454,6 +454,10 @@ int prop_launch(const Layout& L, const double* prep, double* work, int s, int nc
   if (rc != AFQ_OK) return rc;
   base_shape(P, L.npc, N, nc, (int)aK, L.W, BN, err_flag(L, work));
   P.s.a_batched = a_batched;
+  // consecutive launches of one step walk the walkers in opposite directions, so
+  // each starts on the walkers whose VHS, operand pieces and accumulator rows the
+  // previous launch touched last (still in L2)
+  P.s.reverse = (L.tune.prop_order == 0) && (seq & 1);
   P.epi.mode = mode;
   P.epi.npc = L.npc;
   P.epi.N = N;
@@ -623,21 +627,21 @@ static int propagate_one(const Layout& L, const double* prep, double* work, doub
   const long long vbs = (long long)N * L.Kv;
   if (n_exp_terms <= 1) {
     int rc = prop_launch<BN>(L, prep, work, s, nc, PM_Y, 1.f, e, N, L.Nb, N * L.Nb, 0, b0, b1,
-                             nullptr, st);
+                             nullptr, 0, st);
     if (rc != AFQ_OK) return rc;
     return prop_launch<BN>(L, prep, work, s, nc, PM_OUT, 1.f, e, N, L.Nb, N * L.Nb, 0, b1, nullptr,
-                           wk, st);
+                           wk, 1, st);
   }
   // y = e^{-dt h/2} w  -> acc, and [y^T | (i y)^T] into b1
   int rc = prop_launch<BN>(L, prep, work, s, nc, PM_Y, 1.f, e, N, L.Nb, N * L.Nb, 0, b0, b1,
-                           nullptr, st);
+                           nullptr, 0, st);
   if (rc != AFQ_OK) return rc;
   bf16** src = b1;
   bf16** dst = b0;
   for (int n = 1; n < n_exp_terms; ++n) {
     const int mode = (n == n_exp_terms - 1) ? PM_TLAST : PM_T;
     rc = prop_launch<BN>(L, prep, work, s, nc, mode, 1.f / n, v, 2LL * N, L.Kv, vbs, 1, src, dst,
-                         nullptr, st);
+                         nullptr, n, st);
     if (rc != AFQ_OK) return rc;
     bf16** t = src;
     src = dst;
@@ -645,7 +649,7 @@ static int propagate_one(const Layout& L, const double* prep, double* work, doub
   }
   // w' = e^{-dt h/2} (y + sum t_n): B operand holds the finished sum
   return prop_launch<BN>(L, prep, work, s, nc, PM_OUT, 1.f, e, N, L.Nb, N * L.Nb, 0, src, nullptr,
-                         wk, st);
+                         wk, n_exp_terms, st);
 }
 
 int mixed_propagate_walkers(const Layout& L, const double* prep, double* work,

@@ -41,6 +41,7 @@ struct UmmaShape {
   int ngroups;       // 1, or 2: pair 0 (the hi x hi product) accumulates apart from the rest
   int kc;            // K blocks per accumulator chunk (0: the whole K of a tile in one chunk)
   int epi_bytes;     // epilogue scratch per epilogue warpgroup (bytes, multiple of 256)
+  int reverse;       // 1: tiles in reverse order (the last batch first)
   int* err;          // device error flag (set to 1 on a timed-out wait)
 };
 
@@ -155,7 +156,8 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      for (int tile = blockIdx.x; tile < tiles && !*abort_s; tile += gridDim.x) {
+      for (int it_ = blockIdx.x; it_ < tiles && !*abort_s; it_ += gridDim.x) {
+        const int tile = S.reverse ? tiles - 1 - it_ : it_;
         const int nti = tile % S.nt, rest = tile / S.nt;
         const int mti = rest % S.mt, z = rest / S.mt;
         const int b = z / S.ksplit, k0 = (z % S.ksplit) * S.kchunk;
@@ -187,7 +189,8 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
       uint32_t phase = 0;
       int it = 0, t = 0;
       uint32_t uses[NBUF] = {};  // EG > 1: chunks accumulated so far in each buffer
-      for (int tile = blockIdx.x; tile < tiles && !*abort_s; tile += gridDim.x, ++t) {
+      for (int it_ = blockIdx.x; it_ < tiles && !*abort_s; it_ += gridDim.x, ++t) {
+        const int tile = S.reverse ? tiles - 1 - it_ : it_;
         const int k0 = ((tile / (S.nt * S.mt)) % S.ksplit) * S.kchunk;
         const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
         const int kc = S.kc > 0 ? S.kc : KB;
@@ -233,8 +236,9 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
     int it = 0, t = 0;
     uint32_t uses = 0;  // EG = 2: chunks drained from this group's buffer so far
     bool ok = true;
-    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++t) {
+    for (int it_ = blockIdx.x; it_ < tiles && ok; it_ += gridDim.x, ++t) {
       if (EG > 1 && (t % EG) != eg) continue;
+      const int tile = S.reverse ? tiles - 1 - it_ : it_;
       const int nti = tile % S.nt, rest = tile / S.nt;
       const int mti = rest % S.mt, z = rest / S.mt;
       const int k0 = (z % S.ksplit) * S.kchunk;

@@ -287,7 +287,9 @@ typedef struct afq_tuning {
   int32_t max_stages;  /* cap on tcgen05 pipeline stages: 2..8                             */
   int32_t grid_cap;    /* CTAs of the persistent tensor-core kernels: 1..number of SMs     */
   int32_t prop_epi_groups; /* epilogue warpgroups of the tensor-core propagator: 1 to 3    */
-  int32_t reserved[8];
+  int32_t prop_order;  /* propagator tile order: 0 alternate direction per launch (the     */
+                       /* walkers last read stay in L2 for the next launch), 1 forward     */
+  int32_t reserved[7];
 } afq_tuning;
 
 int afq_set_tuning(const afq_dims* d, const afq_tuning* t);
