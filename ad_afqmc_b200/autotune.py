@@ -22,6 +22,12 @@ Knobs (0 = the built-in rule):
                     alternates the direction over the walkers from one launch
                     to the next (each starts where the previous one ended, on
                     data still in L2), 1 always runs forward
+  prop_chunk        1: the propagator accumulates its whole K in one TMEM
+                    chain instead of FP32 round-to-nearest sums of four-block
+                    chunks (frees shared memory for a deeper pipeline: 85 ->
+                    78 us per launch at N=200, W=512, with a block-energy
+                    deviation from FP64 of 0.044 instead of 0.039 mHa).  Not
+                    searched: it changes results beyond the last bits
   grid_cap          CTAs of the persistent kernels (a batch-level knob: a
                     solve alone never gains from fewer CTAs, but overlapping
                     fragments can; ``tune_batch`` sweeps it for a whole batch)

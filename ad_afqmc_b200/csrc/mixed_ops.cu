@@ -470,17 +470,22 @@ int prop_launch(const Layout& L, const double* prep, double* work, int s, int nc
   P.epi.bt_bs = btbs;
   P.epi.wout = wout;
   P.s.ngroups = 2;
-  P.s.kc = 4;
+  // K in chunks of four 64-wide blocks summed in FP32 round-to-nearest through
+  // a shared-memory row per TMEM lane, or (prop_chunk = 1) the whole K in one
+  // TMEM chain, which frees that staging for deeper operand pipelines
+  const bool one_chain = L.tune.prop_chunk == 1;
+  P.s.kc = one_chain ? 0 : 4;
+  const size_t ex = one_chain ? 0 : umma_chunk_stage_bytes(BN);
   // the propagator's epilogue (FP32 accumulator update, next operand pieces)
   // outlasts its MMAs: as many epilogue warpgroups (up to three) as their
   // staging, two pipeline stages and one TMEM buffer per group allow
-  const size_t cs = align256(umma_chunk_stage_bytes(BN));
+  const size_t cs = align256(ex);
   const int want = L.tune.prop_epi_groups ? L.tune.prop_epi_groups : 3;
   if (want >= 3 && 3 * 2 * BN <= 512 && umma_pick_stages(BN, L.npc, L.npc, 3 * cs) >= 2)
-    return run<BN, 3>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
+    return run<BN, 3>(P, ex, st, K_PROP, L.tune);
   if (want >= 2 && umma_pick_stages(BN, L.npc, L.npc, 2 * cs) >= 2)
-    return run<BN, 2>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
-  return run<BN, 1>(P, umma_chunk_stage_bytes(BN), st, K_PROP, L.tune);
+    return run<BN, 2>(P, ex, st, K_PROP, L.tune);
+  return run<BN, 1>(P, ex, st, K_PROP, L.tune);
 }
 
 template <int BN>

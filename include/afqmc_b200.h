@@ -289,7 +289,9 @@ typedef struct afq_tuning {
   int32_t prop_epi_groups; /* epilogue warpgroups of the tensor-core propagator: 1 to 3    */
   int32_t prop_order;  /* propagator tile order: 0 alternate direction per launch (the     */
                        /* walkers last read stay in L2 for the next launch), 1 forward     */
-  int32_t reserved[7];
+  int32_t prop_chunk;  /* propagator K accumulation: 0 chunks of four 64-wide K blocks     */
+                       /* summed in FP32 round-to-nearest, 1 the whole K in one chain     */
+  int32_t reserved[6];
 } afq_tuning;
 
 int afq_set_tuning(const afq_dims* d, const afq_tuning* t);
