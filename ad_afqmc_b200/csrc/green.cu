@@ -315,28 +315,182 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
   }
 }
 
+// Warp 0 of gj_kernel: the pivot among this lane's two candidate rows (lane,
+// lane + 32) and the other lanes': the largest |re|+|im|, the lowest row
+// among equal values (LAPACK izamax).  One 64-bit max-reduction over keys
+// that hold the magnitude's bits above the row number: a non-negative
+// double's bit pattern orders like its value, so the key order is the
+// magnitude order except between values within 128 ulps of each other,
+// which go to the lower row.  Non-candidates have key 0.
+__device__ __forceinline__ int gj_pivot(double2 v0, double2 v1, bool ok0, bool ok1, int lane) {
+  auto key = [](double2 v, int row) -> unsigned long long {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v.x) + fabs(v.y));
+    return (b & ~127ull) | 64ull | (unsigned long long)(63 - row);
+  };
+  unsigned long long k = ok0 ? key(v0, lane) : 0ull;
+  const unsigned long long k1 = ok1 ? key(v1, lane + 32) : 0ull;
+  k = k1 > k ? k1 : k;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long ok = __shfl_xor_sync(0xffffffffu, k, o);
+    k = ok > k ? ok : k;
+  }
+  return 63 - (int)(k & 63ull);
+}
+
 // Gauss-Jordan inverse and det of S = C^T W held in sbuf, one CTA per
-// (walker, sector), in place (the arithmetic of the whole-computation mode).
-// Only S, its pivot column and the permutation live in shared memory, so
-// several CTAs share an SM and hide each other's barrier latency.
+// (walker, sector), in place, with one block barrier per elimination step
+// (partial pivoting, pivot = largest |re|+|im| in the column).
+//  * Rows are never swapped: the pivot row r_k of step k stays in place and
+//    the inverse is unscrambled once at the end, S^-1[i][r_k] = X[r_i][k].
+//  * Step k reads buffer k & 1 and writes the other, so nothing is read after
+//    it was overwritten within a step.  Rows are stored with an odd stride
+//    (ld = no | 1 double2), so a warp reading a column hits distinct banks.
+//  * During step k warp 0 computes the new pivot column k+1, its pivot (over
+//    the rows not yet used), the reciprocal and the scaled new pivot row,
+//    which every thread reads in step k+1; warps 1..7 update all other
+//    elements.  det = product of the pivots times the permutation's sign.
+// At most 64 rows (no <= 64, checked by the caller).
 __global__ void __launch_bounds__(kGreenThreads, 4)
-    gj_kernel(int W, int no0, int no1, double* sbuf, long long sstride, double* wscal) {
+    gj_kernel(int W, int no0, int no1, double* sbuf, long long sstride, int bstride, double* wscal) {
   extern __shared__ double2 gsm[];
   const int w = blockIdx.x, sct = blockIdx.y;
   const int no = sct ? no1 : no0;
-  double2* S = gsm;
-  double2* colk = S + sstride;
-  __shared__ int perm[64];
-  __shared__ double2 ipk_s;
-  double2* g = reinterpret_cast<double2*>(sbuf) + ((long long)sct * W + w) * sstride;
+  const int ld = no | 1;
   const int nn = no * no;
-  for (int e = threadIdx.x; e < nn; e += kGreenThreads) S[e] = g[e];
+  double2* const buf0 = gsm;
+  double2* const buf1 = gsm + bstride;
+  double2* const prow = gsm + 2 * bstride;  // [2][64]: scaled pivot row of the step, by parity
+  __shared__ double2 ipks[2];
+  __shared__ int piv[64];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double2* g = reinterpret_cast<double2*>(sbuf) + ((long long)sct * W + w) * sstride;
+  for (int e = tid; e < nn; e += kGreenThreads) {
+    const int i = e / no;
+    buf0[i * ld + (e - i * no)] = g[e];
+  }
   __syncthreads();
-  const double2 det = gauss_jordan_cta(S, colk, perm, &ipk_s, no);
-  for (int e = threadIdx.x; e < nn; e += kGreenThreads) g[e] = S[e];
-  if (threadIdx.x == 0 && wscal) {
-    wscal[(long long)w * 16 + 4 + 2 * sct] = det.x;
-    wscal[(long long)w * 16 + 5 + 2 * sct] = det.y;
+
+  const double2 zero = make_double2(0.0, 0.0);
+  const bool in0 = lane < no, in1 = lane + 32 < no;
+  bool used0 = false, used1 = false;  // warp 0: rows lane, lane + 32 already pivots
+  double2 det = make_double2(1.0, 0.0);
+  if (warp == 0) {  // pivot of column 0 and its scaled row
+    const double2 v0 = in0 ? buf0[lane * ld] : zero, v1 = in1 ? buf0[(lane + 32) * ld] : zero;
+    const int r = gj_pivot(v0, v1, in0, in1, lane);
+    const double2 p = buf0[r * ld];
+    const double inv = 1.0 / (p.x * p.x + p.y * p.y);
+    const double2 ipk = make_double2(p.x * inv, -p.y * inv);
+    if (lane == (r & 31)) (r < 32 ? used0 : used1) = true;
+    for (int j = lane; j < no; j += 32) prow[j] = (j == 0) ? ipk : cmul(buf0[r * ld + j], ipk);
+    if (lane == 0) {
+      piv[0] = r;
+      ipks[0] = ipk;
+      det = p;
+    }
+  }
+  __syncthreads();
+
+  // warps 1..7: fixed element walk e = tid - 32 + q * 224, (i, j) advanced incrementally
+  constexpr int TW = kGreenThreads - 32;
+  const int nd = no > 0 ? no : 1;
+  const int di = TW / nd, dj = TW - di * nd;
+  for (int k = 0; k < no; ++k) {
+    const int cur = k & 1;
+    const double2* src = cur ? buf1 : buf0;
+    double2* dst = cur ? buf0 : buf1;
+    const double2* pr = prow + cur * 64;
+    const int r = piv[k];
+    const double2 ipk = ipks[cur];
+    const int c = k + 1;
+    if (warp == 0) {
+      if (c < no) {
+        // new column c, then the next pivot among the unused rows
+        double2 v0 = zero, v1 = zero;
+        const double2 prc = pr[c];
+        if (in0) {
+          const int i = lane;
+          v0 = (i == r) ? prc : csub(src[i * ld + c], cmul(src[i * ld + k], prc));
+          dst[i * ld + c] = v0;
+        }
+        if (in1) {
+          const int i = lane + 32;
+          v1 = (i == r) ? prc : csub(src[i * ld + c], cmul(src[i * ld + k], prc));
+          dst[i * ld + c] = v1;
+        }
+        const int rn = gj_pivot(v0, v1, in0 && !used0, in1 && !used1, lane);
+        __syncwarp();
+        const double2 p = dst[rn * ld + c];
+        const double inv = 1.0 / (p.x * p.x + p.y * p.y);
+        const double2 ipn = make_double2(p.x * inv, -p.y * inv);
+        if (lane == (rn & 31)) (rn < 32 ? used0 : used1) = true;
+        // the new pivot row after this step, scaled by 1/p
+        const double2 f = src[rn * ld + k];
+        double2* pn = prow + (cur ^ 1) * 64;
+        for (int j = lane; j < no; j += 32) {
+          double2 v;
+          if (j == c) {
+            v = ipn;
+          } else if (j == k) {
+            const double2 t0 = cmul(f, ipk);
+            v = cmul(make_double2(-t0.x, -t0.y), ipn);
+          } else {
+            v = cmul(csub(src[rn * ld + j], cmul(f, pr[j])), ipn);
+          }
+          pn[j] = v;
+        }
+        if (lane == 0) {
+          piv[c] = rn;
+          ipks[cur ^ 1] = ipn;
+          det = cmul(det, p);
+        }
+      }
+    } else {
+      int e = tid - 32;
+      int i = e / nd, j = e - (e / nd) * nd;
+      for (; e < nn; e += TW) {
+        if (j != c) {
+          double2 v;
+          if (i == r) {
+            v = (j == k) ? ipk : pr[j];
+          } else {
+            const double2 f = src[i * ld + k];
+            if (j == k) {
+              const double2 t0 = cmul(f, ipk);
+              v = make_double2(-t0.x, -t0.y);
+            } else {
+              v = csub(src[i * ld + j], cmul(f, pr[j]));
+            }
+          }
+          dst[i * ld + j] = v;
+        }
+        i += di;
+        j += dj;
+        if (j >= no) { j -= no; ++i; }
+      }
+    }
+    __syncthreads();
+  }
+  // unscramble: S^-1[i][r_k] = X[r_i][k]
+  const double2* X = (no & 1) ? buf1 : buf0;
+  for (int e = tid; e < nn; e += kGreenThreads) {
+    const int i = e / no, k = e - (e / no) * no;
+    g[i * no + piv[k]] = X[piv[i] * ld + k];
+  }
+  if (tid == 0) {
+    // sign of the permutation k -> r_k: (-1)^(no - cycles)
+    unsigned long long seen = 0ull;
+    int cycles = 0;
+    for (int s0 = 0; s0 < no; ++s0) {
+      if (seen >> s0 & 1ull) continue;
+      ++cycles;
+      for (int t = s0; !(seen >> t & 1ull); t = piv[t]) seen |= 1ull << t;
+    }
+    if ((no - cycles) & 1) det = make_double2(-det.x, -det.y);
+    if (wscal) {
+      wscal[(long long)w * 16 + 4 + 2 * sct] = det.x;
+      wscal[(long long)w * 16 + 5 + 2 * sct] = det.y;
+    }
   }
 }
 
@@ -379,12 +533,14 @@ cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   // S into a.sbuf; warp-level inverse and det; Theta and its outputs
   green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 1);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const size_t gsmem = (size_t(a.sstride) + 64) * sizeof(double2);
+  // two row-padded copies of S (row stride nomax | 1) and two scaled pivot rows
+  const int bstride = nomax * (nomax | 1);
+  const size_t gsmem = (2 * size_t(bstride) + 128) * sizeof(double2);
   if ((e = cudaFuncSetAttribute(gj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem)) !=
       cudaSuccess)
     return e;
   gj_kernel<<<grid, kGreenThreads, gsmem, st>>>(a.W, a.sec[0].no, a.ns > 1 ? a.sec[1].no : 0,
-                                                a.sbuf, a.sstride, a.wscal);
+                                                a.sbuf, a.sstride, bstride, a.wscal);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 2);
   return cudaGetLastError();
