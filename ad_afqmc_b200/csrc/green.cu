@@ -22,6 +22,24 @@ namespace {
 constexpr int kGreenThreads = 256;
 constexpr int kRowChunk = 32;
 
+// asynchronous global -> shared copies (Ampere-style cp.async): the next
+// chunk of walker rows streams in while the current one is multiplied
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most one group (the newest) of this thread's copies is in flight
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 // Gauss-Jordan inverse with partial pivoting of the No x No complex S in
 // shared memory, in place, by the whole CTA (kGreenThreads threads); returns
 // det S in thread 0.
@@ -118,9 +136,10 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
 
   double2* S = sm;                          // no*no
   double2* colk = S + no * no;              // 64
-  double2* stage = colk + 64;               // kRowChunk*no   (walker rows, C^T W phase)
-  double* moc = reinterpret_cast<double*>(stage + kRowChunk * no);  // kRowChunk*no
-  double2* tstage = reinterpret_cast<double2*>(moc + kRowChunk * no);  // kRowChunk*(no+1)
+  // two buffers each of walker rows and trial rows (chunk c in buffer c & 1)
+  double2* stage = colk + 64;                                            // 2 x kRowChunk*no
+  double* moc = reinterpret_cast<double*>(stage + 2 * kRowChunk * no);   // 2 x kRowChunk*no
+  double2* tstage = reinterpret_cast<double2*>(moc + 2 * kRowChunk * no);  // kRowChunk*(no+1)
   const int ts = no + 1;  // padded row stride of tstage (conflict-free column reads)
   __shared__ double red[2 * (T / 32)];
   __shared__ int perm[64];
@@ -136,7 +155,18 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
   const int warp = tid >> 5, lane = tid & 31;
   const int nc2 = 2 * no;
   const int mtiles = (no + 7) >> 3, ntiles = (nc2 + 7) >> 3;  // <= 8, <= 16
-  const double* stageD = reinterpret_cast<const double*>(stage);
+  const int nchunks = (N + kRowChunk - 1) / kRowChunk;
+  // chunk c of the walker rows (and, with_mo, of the trial rows) into buffer c & 1
+  auto load_chunk = [&](int c, bool with_mo) {
+    const int p0 = c * kRowChunk, rows = min(kRowChunk, N - p0);
+    double2* st = stage + (c & 1) * kRowChunk * no;
+    double* mc = moc + (c & 1) * kRowChunk * no;
+    for (int e = tid; e < rows * no; e += T) {
+      cp_async16(&st[e], &Wg[(long long)p0 * no + e]);
+      if (with_mo) cp_async8(&mc[e], &S_.mo[(long long)p0 * no + e]);
+    }
+    cp_async_commit();
+  };
   double2* sg = a.sbuf ? reinterpret_cast<double2*>(a.sbuf) + ((long long)sct * a.W + w) * a.sstride
                        : nullptr;
   const int npairs = no * no;
@@ -146,13 +176,15 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
   for (int sl = 0; sl < 2; ++sl)
 #pragma unroll
     for (int mi = 0; mi < 8; ++mi) sacc[sl][mi][0] = sacc[sl][mi][1] = 0.0;
-  for (int p0 = 0; p0 < N; p0 += kRowChunk) {
-    const int rows = min(kRowChunk, N - p0);
-    for (int e = tid; e < rows * no; e += T) {
-      stage[e] = Wg[(long long)p0 * no + e];
-      moc[e] = S_.mo[(long long)p0 * no + e];
-    }
+  load_chunk(0, true);
+  for (int c = 0; c < nchunks; ++c) {
+    const int p0 = c * kRowChunk, rows = min(kRowChunk, N - p0);
+    if (c + 1 < nchunks) load_chunk(c + 1, true);
+    else cp_async_commit();  // an empty group keeps the wait count uniform
+    cp_async_wait1();
     __syncthreads();
+    const double* stageD = reinterpret_cast<const double*>(stage + (c & 1) * kRowChunk * no);
+    const double* mocc = moc + (c & 1) * kRowChunk * no;
     for (int kk = 0; kk < rows; kk += 4) {
       const int kr = kk + (lane & 3);
       const bool kin = kr < rows;
@@ -160,7 +192,7 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
 #pragma unroll
       for (int mi = 0; mi < 8; ++mi) {
         const int m = mi * 8 + (lane >> 2);
-        afr[mi] = (mi < mtiles && kin && m < no) ? moc[kr * no + m] : 0.0;
+        afr[mi] = (mi < mtiles && kin && m < no) ? mocc[kr * no + m] : 0.0;
       }
 #pragma unroll
       for (int sl = 0; sl < 2; ++sl) {
@@ -221,11 +253,15 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
   double* gim = a.gpl ? a.gpl + (2LL * w + 1) * a.ldg + S_.koff : nullptr;
   const bool gb = a.gplb[0] != nullptr;
   const bool tb = S_.gtb[0] != nullptr;
-  for (int p0 = 0; p0 < N; p0 += kRowChunk) {
-    const int rows = min(kRowChunk, N - p0);
-    // walker rows of this chunk into shared memory
-    for (int e = tid; e < rows * no; e += T) stage[e] = Wg[(long long)p0 * no + e];
+  load_chunk(0, false);
+  for (int c = 0; c < nchunks; ++c) {
+    const int p0 = c * kRowChunk, rows = min(kRowChunk, N - p0);
+    // walker rows of the next chunk stream in while this one is processed
+    if (c + 1 < nchunks) load_chunk(c + 1, false);
+    else cp_async_commit();
+    cp_async_wait1();
     __syncthreads();
+    const double* stageD = reinterpret_cast<const double*>(stage + (c & 1) * kRowChunk * no);
     // Theta rows (N x 2No real) = W rows (N x 2No) times the real form of
     // S^-1: R[2i][2j] = R[2i+1][2j+1] = Re s_ij, R[2i][2j+1] = Im s_ij,
     // R[2i+1][2j] = -Im s_ij, generated in the B fragments
@@ -515,8 +551,8 @@ __global__ void ovlp_combine_kernel(int W, int ns, int mult, const double* wscal
 cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   int nomax = 0;
   for (int s = 0; s < a.ns; ++s) nomax = a.sec[s].no > nomax ? a.sec[s].no : nomax;
-  const size_t smem = (size_t(nomax) * nomax + 64 + kRowChunk * nomax) * sizeof(double2) +
-                      size_t(kRowChunk) * nomax * sizeof(double) +
+  const size_t smem = (size_t(nomax) * nomax + 64 + 2 * kRowChunk * nomax) * sizeof(double2) +
+                      2 * size_t(kRowChunk) * nomax * sizeof(double) +
                       size_t(kRowChunk) * (nomax + 1) * sizeof(double2);
   cudaError_t e = cudaFuncSetAttribute(green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
