@@ -136,9 +136,14 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
 
   double2* S = sm;                          // no*no
   double2* colk = S + no * no;              // 64
-  // two buffers each of walker rows and trial rows (chunk c in buffer c & 1)
-  double2* stage = colk + 64;                                            // 2 x kRowChunk*no
-  double* moc = reinterpret_cast<double*>(stage + 2 * kRowChunk * no);   // 2 x kRowChunk*no
+  // two buffers each of walker rows and trial rows (chunk c in buffer c & 1);
+  // walker rows at a stride of sd doubles, sd = 4 (mod 16): the 8-byte
+  // fragment loads of a warp (8 rows x 4 columns, or 4 rows x 8 columns) then
+  // take the minimum two shared-memory wavefronts
+  const int nc2_ = 2 * no;
+  const int sd = nc2_ + ((20 - nc2_ % 16) % 16);
+  double2* stage = colk + 64;                                            // 2 x kRowChunk*sd/2
+  double* moc = reinterpret_cast<double*>(stage + kRowChunk * sd);        // 2 x kRowChunk*no
   double2* tstage = reinterpret_cast<double2*>(moc + 2 * kRowChunk * no);  // kRowChunk*(no+1)
   const int ts = no + 1;  // padded row stride of tstage (conflict-free column reads)
   __shared__ double red[2 * (T / 32)];
@@ -159,10 +164,11 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
   // chunk c of the walker rows (and, with_mo, of the trial rows) into buffer c & 1
   auto load_chunk = [&](int c, bool with_mo) {
     const int p0 = c * kRowChunk, rows = min(kRowChunk, N - p0);
-    double2* st = stage + (c & 1) * kRowChunk * no;
+    double2* st = stage + (c & 1) * kRowChunk * (sd / 2);
     double* mc = moc + (c & 1) * kRowChunk * no;
     for (int e = tid; e < rows * no; e += T) {
-      cp_async16(&st[e], &Wg[(long long)p0 * no + e]);
+      const int r = e / no;
+      cp_async16(&st[r * (sd / 2) + (e - r * no)], &Wg[(long long)p0 * no + e]);
       if (with_mo) cp_async8(&mc[e], &S_.mo[(long long)p0 * no + e]);
     }
     cp_async_commit();
@@ -183,7 +189,7 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
     else cp_async_commit();  // an empty group keeps the wait count uniform
     cp_async_wait1();
     __syncthreads();
-    const double* stageD = reinterpret_cast<const double*>(stage + (c & 1) * kRowChunk * no);
+    const double* stageD = reinterpret_cast<const double*>(stage + (c & 1) * kRowChunk * (sd / 2));
     const double* mocc = moc + (c & 1) * kRowChunk * no;
     for (int kk = 0; kk < rows; kk += 4) {
       const int kr = kk + (lane & 3);
@@ -199,7 +205,7 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
         const int ni = warp + sl * 8;
         if (ni < ntiles) {  // warp-uniform
           const int n = ni * 8 + (lane >> 2);
-          const double b = (kin && n < nc2) ? stageD[kr * nc2 + n] : 0.0;
+          const double b = (kin && n < nc2) ? stageD[kr * sd + n] : 0.0;
 #pragma unroll
           for (int mi = 0; mi < 8; ++mi)
             if (mi < mtiles) dmma_8x8x4(sacc[sl][mi][0], sacc[sl][mi][1], afr[mi], b);
@@ -261,7 +267,7 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
     else cp_async_commit();
     cp_async_wait1();
     __syncthreads();
-    const double* stageD = reinterpret_cast<const double*>(stage + (c & 1) * kRowChunk * no);
+    const double* stageD = reinterpret_cast<const double*>(stage + (c & 1) * kRowChunk * (sd / 2));
     // Theta rows (N x 2No real) = W rows (N x 2No) times the real form of
     // S^-1: R[2i][2j] = R[2i+1][2j+1] = Re s_ij, R[2i][2j+1] = Im s_ij,
     // R[2i+1][2j] = -Im s_ij, generated in the B fragments
@@ -279,7 +285,7 @@ __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int m
 #pragma unroll
         for (int ri = 0; ri < 4; ++ri) {
           const int r = ri * 8 + (lane >> 2);
-          afr[ri] = (ri < rtiles && kin && r < rows) ? stageD[r * nc2 + k] : 0.0;
+          afr[ri] = (ri < rtiles && kin && r < rows) ? stageD[r * sd + k] : 0.0;
         }
 #pragma unroll
         for (int sl = 0; sl < 2; ++sl) {
@@ -551,7 +557,9 @@ __global__ void ovlp_combine_kernel(int W, int ns, int mult, const double* wscal
 cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   int nomax = 0;
   for (int s = 0; s < a.ns; ++s) nomax = a.sec[s].no > nomax ? a.sec[s].no : nomax;
-  const size_t smem = (size_t(nomax) * nomax + 64 + 2 * kRowChunk * nomax) * sizeof(double2) +
+  const int sdmax = 2 * nomax + ((20 - (2 * nomax) % 16) % 16);  // padded walker-row stride (doubles)
+  const size_t smem = (size_t(nomax) * nomax + 64) * sizeof(double2) +
+                      2 * size_t(kRowChunk) * sdmax * sizeof(double) +
                       2 * size_t(kRowChunk) * nomax * sizeof(double) +
                       size_t(kRowChunk) * (nomax + 1) * sizeof(double2);
   cudaError_t e = cudaFuncSetAttribute(green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
