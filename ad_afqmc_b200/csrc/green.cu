@@ -433,10 +433,14 @@ __global__ void __launch_bounds__(kGreenThreads, 4)
   }
   __syncthreads();
 
-  // warps 1..7: fixed element walk e = tid - 32 + q * 224, (i, j) advanced incrementally
+  // warps 1..7: thread tid - 32 = g * no + j owns column j, rows g, g + G, ...
+  // (G = 224 / no row groups; threads beyond G * no idle)
   constexpr int TW = kGreenThreads - 32;
   const int nd = no > 0 ? no : 1;
-  const int di = TW / nd, dj = TW - di * nd;
+  const int G = TW / nd;
+  const int tu = tid - 32;
+  const int jc = tu % nd, g0 = tu / nd;
+  const bool upd = warp > 0 && g0 < G;
   for (int k = 0; k < no; ++k) {
     const int cur = k & 1;
     const double2* src = cur ? buf1 : buf0;
@@ -487,28 +491,17 @@ __global__ void __launch_bounds__(kGreenThreads, 4)
           det = cmul(det, p);
         }
       }
-    } else {
-      int e = tid - 32;
-      int i = e / nd, j = e - (e / nd) * nd;
-      for (; e < nn; e += TW) {
-        if (j != c) {
-          double2 v;
-          if (i == r) {
-            v = (j == k) ? ipk : pr[j];
-          } else {
-            const double2 f = src[i * ld + k];
-            if (j == k) {
-              const double2 t0 = cmul(f, ipk);
-              v = make_double2(-t0.x, -t0.y);
-            } else {
-              v = csub(src[i * ld + j], cmul(f, pr[j]));
-            }
-          }
-          dst[i * ld + j] = v;
+    } else if (upd && jc != c) {
+      const int j = jc;
+      if (j == k) {  // the pivot column: -f / p, and 1 / p in the pivot row
+        for (int i = g0; i < no; i += G) {
+          const double2 t0 = cmul(src[i * ld + k], ipk);
+          dst[i * ld + j] = (i == r) ? ipk : make_double2(-t0.x, -t0.y);
         }
-        i += di;
-        j += dj;
-        if (j >= no) { j -= no; ++i; }
+      } else {
+        const double2 prj = pr[j];
+        for (int i = g0; i < no; i += G)
+          dst[i * ld + j] = (i == r) ? prj : csub(src[i * ld + j], cmul(src[i * ld + k], prj));
       }
     }
     __syncthreads();

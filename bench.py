@@ -143,7 +143,7 @@ FP64_PEAK_TFLOPS = 35.47
 # DRAM bytes (read + written) per propagator launch, mean over the 7 launches
 # of one step, from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
 # bench workload (N=200, No=40, G=1000, 512 walkers, mixed).
-PROP_DRAM_BYTES_PER_LAUNCH = 256684727
+PROP_DRAM_BYTES_PER_LAUNCH = 257510875
 
 
 def main():
