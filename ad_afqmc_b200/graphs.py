@@ -35,14 +35,19 @@ from .walkers import UHFWalkers
 
 class BlockGraph:
     def __init__(self, ham, ham_data, prop, trial, wave_data, prop_data, n_prop_steps: int = 10,
-                 update_estimate: bool = True, reconfigure: bool = True, lno: bool = False):
+                 update_estimate: bool = True, reconfigure: bool = True, lno: bool = False,
+                 external_fields: bool = False):
         """reconfigure=False leaves the comb (and the overlaps of the new
         walkers) out of the recorded block, for callers that reconfigure
         across ranks after each replay; update_estimate=False leaves out the
         e_estimate update (a caller with several ranks updates it from the
         all-reduced block energy).  lno=True records the block end of
         sampler_lno (sampling.py:586-631) for an rhf_lno trial and restricted
-        walkers: block_out then holds (energy, weight, orbital energy)."""
+        walkers: block_out then holds (energy, weight, orbital energy).
+        external_fields=True leaves the field draw out of the recorded block:
+        the caller writes each block's fields into ``self.fields`` (S, W, G)
+        before the replay (``HostFieldBlocks`` streams them from host memory);
+        zeta still comes from the device stream."""
         self.prop, self.trial, self.wave_data, self.ham_data = prop, trial, wave_data, ham_data
         self.eng = prop.engine(ham_data, trial, wave_data)
         if not self.eng.has_prop:
@@ -64,6 +69,7 @@ class BlockGraph:
         self.counter = torch.tensor([key.counter], dtype=torch.int64, device=dev)
         self.zeta = torch.zeros(1, dtype=torch.float64, device=dev)
         self.lno = bool(lno)
+        self.external_fields = bool(external_fields)
         self.block_out = torch.zeros(3 if self.lno else 2, dtype=torch.float64, device=dev)
         if self.lno:
             if isinstance(w, UHFWalkers) or "prjlo" not in wave_data:
@@ -88,8 +94,9 @@ class BlockGraph:
         sc[1].copy_(sc[0])  # pop_control_ene_shift = e_estimate
         sc[2].zero_()       # n_killed_walkers
         n0 = _lib.launch_count()
-        _lib.check(lib.afq_normal_fields_dev(self.fields.data_ptr(), self.fields.numel(), self.seed,
-                                             self.counter.data_ptr(), stream), "afq_normal_fields_dev")
+        if not self.external_fields:
+            _lib.check(lib.afq_normal_fields_dev(self.fields.data_ptr(), self.fields.numel(), self.seed,
+                                                 self.counter.data_ptr(), stream), "afq_normal_fields_dev")
         st = make_state(pd)  # GREEN_CURRENT clear: the first step computes G
         p, w, wb = eng.handle
         for s in range(self.S):
@@ -232,3 +239,64 @@ class BatchGraph:
     @property
     def launches_per_block(self) -> int:
         return sum(b.launches_per_block for b in self.blocks)
+
+
+class HostFieldBlocks:
+    """Blocks of a BlockGraph recorded with external_fields=True, fed from
+    host memory: the fields of the next block are uploaded on a copy stream
+    (into one of two device staging buffers) while the current block runs,
+    then copied into the graph's field buffer just before its replay.  Each
+    block's results (energy, weight and the walker weights) are read back to
+    a pinned host buffer.
+
+        runner = HostFieldBlocks(bg)
+        runner.upload(fields_of_block_0)          # pinned (S, W, G) float64
+        for b in range(n):
+            out = runner.run(fields_of_block_b_plus_1)  # numpy (energy, weight, weights...)
+    """
+
+    def __init__(self, bg: BlockGraph):
+        if not bg.external_fields or bg.graph is None:
+            raise _lib.AfqError("HostFieldBlocks needs a captured BlockGraph with external_fields=True")
+        self.bg = bg
+        self.copy_stream = torch.cuda.Stream()
+        self.staging = [torch.empty_like(bg.fields) for _ in range(2)]
+        self.ready = [torch.cuda.Event() for _ in range(2)]
+        self.free = [torch.cuda.Event() for _ in range(2)]
+        self.n = 0
+        W = bg.prop.n_walkers
+        self.out_host = torch.empty(2 + W, dtype=torch.float64).pin_memory()
+        self.h2d_bytes = bg.fields.numel() * bg.fields.element_size()
+        self.d2h_bytes = self.out_host.numel() * self.out_host.element_size()
+
+    def upload(self, host_fields: torch.Tensor) -> None:
+        """Queue the upload of the fields of block ``self.n`` (the next to run)."""
+        self._upload(self.n, host_fields)
+
+    def _upload(self, block: int, host_fields: torch.Tensor) -> None:
+        i = block % 2
+        if tuple(host_fields.shape) != tuple(self.bg.fields.shape):
+            raise _lib.AfqError(f"fields must have shape {tuple(self.bg.fields.shape)}")
+        with torch.cuda.stream(self.copy_stream):
+            self.copy_stream.wait_event(self.free[i])  # the previous user of this buffer copied it out
+            self.staging[i].copy_(host_fields, non_blocking=True)
+            self.ready[i].record(self.copy_stream)
+
+    def run(self, next_host_fields: Optional[torch.Tensor] = None):
+        """Run block ``self.n`` (its fields must have been uploaded), queue
+        the upload of the next block's fields, and return the block's
+        (energy, weight) followed by the walker weights as a numpy array."""
+        i = self.n % 2
+        cur = torch.cuda.current_stream()
+        cur.wait_event(self.ready[i])
+        self.bg.fields.copy_(self.staging[i])
+        self.free[i].record(cur)
+        self.bg.replay()
+        if next_host_fields is not None:
+            self._upload(self.n + 1, next_host_fields)
+        self.out_host[:2].copy_(self.bg.block_out[:2], non_blocking=True)
+        self.out_host[2:].copy_(self.bg.pd["weights"], non_blocking=True)
+        cur.synchronize()
+        self.n += 1
+        return self.out_host.numpy().copy()
+

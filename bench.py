@@ -350,31 +350,53 @@ def main():
             def uniform(self):
                 return 0.5
 
-        smp_e2e = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1, field_source=PinnedSource())
-        out_host = torch.empty(W + 1, dtype=torch.float64).pin_memory()
+        if world == 1:
+            # the block as one CUDA graph fed from host memory (graphs.HostFieldBlocks):
+            # every block uploads its fields from the pinned buffer (on a copy stream,
+            # overlapping the previous block) and reads (energy, weight, weights) back
+            from ad_afqmc_b200.graphs import BlockGraph, HostFieldBlocks
 
-        def e2e_block(pd):
-            e, pd = smp_e2e.propagate_phaseless(ham, ham_data, prop, pd, trial, wave)
-            out_host[0].copy_(e, non_blocking=True)
-            out_host[1:].copy_(pd["weights"], non_blocking=True)
-            torch.cuda.current_stream().synchronize()
-            pd["e_estimate"] = 0.9 * pd["e_estimate"] + 0.1 * e
-            return pd
+            bg = BlockGraph(ham, ham_data, prop, trial, wave, pd, n_prop_steps=S, external_fields=True)
+            bg.fields.copy_(host_fields)
+            bg.capture(warmup=1)
+            runner = HostFieldBlocks(bg)
+            runner.upload(host_fields)
+            runner.run(host_fields)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                runner.run(host_fields)
+            torch.cuda.synchronize()
+            t_e2e = time.perf_counter() - t0
+            out_numel = runner.out_host.numel()
+        else:
+            smp_e2e = sampling.sampler(n_prop_steps=S, n_ene_blocks=1, n_sr_blocks=1,
+                                       field_source=PinnedSource())
+            out_host = torch.empty(W + 1, dtype=torch.float64).pin_memory()
 
-        pd = e2e_block(pd)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
+            def e2e_block(pd):
+                e, pd = smp_e2e.propagate_phaseless(ham, ham_data, prop, pd, trial, wave)
+                out_host[0].copy_(e, non_blocking=True)
+                out_host[1:].copy_(pd["weights"], non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+                pd["e_estimate"] = 0.9 * pd["e_estimate"] + 0.1 * e
+                return pd
+
             pd = e2e_block(pd)
-        torch.cuda.synchronize()
-        t_e2e = time.perf_counter() - t0
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                pd = e2e_block(pd)
+            torch.cuda.synchronize()
+            t_e2e = time.perf_counter() - t0
+            out_numel = out_host.numel()
         if world > 1:
             t = torch.tensor([t_e2e], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             t_e2e = float(t.item())
         e2e = {"value": world * W * S * args.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": int(host_fields.numel() * 8),
-               "d2h_bytes_per_step": int(out_host.numel() * 8)}
+               "d2h_bytes_per_step": int(out_numel * 8)}
 
     if rank != 0:
         if world > 1:

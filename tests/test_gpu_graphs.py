@@ -67,3 +67,36 @@ def test_batch_graph_equals_solves_alone():
     for b, ref in zip(blocks, alone):
         for x, y in zip(_state(b), ref):
             assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_host_fed_blocks_equal_device_fields(precision):
+    """A block recorded with external_fields=True and fed the same fields from
+    pinned host memory (HostFieldBlocks: uploads overlapped with the previous
+    block) gives the block energy and weight of the block that drew them on
+    the device, bit for bit, over several blocks (no comb, whose zeta comes
+    from the device stream)."""
+    from ad_afqmc_b200 import graphs
+
+    def parts():
+        sys_ = make_system(24, (6, 6), 96, seed=9, trial="rhf", chol_scale=0.25)
+        d_trial, d_ham, d_wave, d_prop, ham = device_system(sys_, "restricted", 0.005, 32, precision=precision)
+        pd = d_prop.init_prop_data(d_trial, d_wave, d_ham, 9)
+        return ham, d_ham, d_prop, d_trial, d_wave, pd
+
+    a = graphs.BlockGraph(*parts(), n_prop_steps=4, reconfigure=False).capture(warmup=0)
+    b = graphs.BlockGraph(*parts(), n_prop_steps=4, reconfigure=False, external_fields=True)
+    n = 4
+    host = [torch.empty(a.fields.shape, dtype=torch.float64).pin_memory() for _ in range(n)]
+    ea = []
+    for k in range(n):
+        ea.append(a.replay()[:2].cpu().numpy().copy())
+        host[k].copy_(a.fields.cpu())
+    b.fields.copy_(host[0])
+    b.capture(warmup=0)
+    runner = graphs.HostFieldBlocks(b)
+    runner.upload(host[0])
+    eb = [runner.run(host[k + 1] if k + 1 < n else None)[:2] for k in range(n)]
+    for x, y in zip(ea, eb):
+        assert np.array_equal(x, y)
+    assert runner.h2d_bytes == host[0].numel() * 8
