@@ -264,6 +264,7 @@ class HostFieldBlocks:
         self.ready = [torch.cuda.Event() for _ in range(2)]
         self.free = [torch.cuda.Event() for _ in range(2)]
         self.n = 0
+        self.uploaded = -1  # last block whose fields were queued
         W = bg.prop.n_walkers
         self.out_host = torch.empty(2 + W, dtype=torch.float64).pin_memory()
         self.h2d_bytes = bg.fields.numel() * bg.fields.element_size()
@@ -277,6 +278,9 @@ class HostFieldBlocks:
         i = block % 2
         if tuple(host_fields.shape) != tuple(self.bg.fields.shape):
             raise _lib.AfqError(f"fields must have shape {tuple(self.bg.fields.shape)}")
+        if block != self.uploaded + 1:
+            raise _lib.AfqError(f"fields of block {block} queued out of order (last queued: {self.uploaded})")
+        self.uploaded = block
         with torch.cuda.stream(self.copy_stream):
             self.copy_stream.wait_event(self.free[i])  # the previous user of this buffer copied it out
             self.staging[i].copy_(host_fields, non_blocking=True)
@@ -286,6 +290,8 @@ class HostFieldBlocks:
         """Run block ``self.n`` (its fields must have been uploaded), queue
         the upload of the next block's fields, and return the block's
         (energy, weight) followed by the walker weights as a numpy array."""
+        if self.uploaded < self.n:
+            raise _lib.AfqError(f"the fields of block {self.n} were not uploaded")
         i = self.n % 2
         cur = torch.cuda.current_stream()
         cur.wait_event(self.ready[i])
