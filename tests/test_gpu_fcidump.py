@@ -99,6 +99,7 @@ def test_run_afqmc_driver_options(calc_dir, precision):
     e, err = launch_script.run_afqmc(options, tmpdir=d)
     e_ref = meta["reference_values"]["afqmc_energy_1proc"][0]
     err = float(err) if err is not None and np.isfinite(err) else 0.0
+    print(f"run_afqmc ({precision}): E = {e:.6f} +- {err:.6f} Ha; reference run {e_ref:.6f} Ha")
     # two independent stochastic runs of 50 walkers x 5000 steps: a few mHa apart at most
     assert abs(e - e_ref) < max(0.01, 5.0 * err), (e, err, e_ref)
     assert e < e_uhf - 0.05
