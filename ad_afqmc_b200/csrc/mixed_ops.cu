@@ -138,11 +138,7 @@ struct VhsEpiU {
   long long ld, wstride;
   template <int BN>
   __device__ void tile(int, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
-                       uint8_t* escr) const {
-    if (src.srow && (N & 15) == 0 && (ld & 7) == 0 && (wstride & 7) == 0) {
-      tile_rows16<BN>(mti, nti, row, s, reinterpret_cast<const float*>(escr));
-      return;
-    }
+                       uint8_t*) const {
     const int q = mti * s.a_step + row;  // q = p*N + r
     const int p = q / N, r = q - (q / N) * N;
 #pragma unroll 1
@@ -160,56 +156,6 @@ struct VhsEpiU {
         }
       }
     }
-  }
-
-  // The tile's finished sums are in the group's shared rows (128 rows of BN + 1
-  // floats): the 128 epilogue threads write them together, each item 16
-  // consecutive rows q of one column n, which are 16 consecutive r of one VHS
-  // row (N is a multiple of 16), so every piece goes out as one 32-byte sector
-  // instead of 16 two-byte stores.  Same pieces as put_pieces_f, bit for bit.
-  template <int BN>
-  __device__ void tile_rows16(int mti, int nti, int row, const UmmaShape& s, const float* rows) const {
-    named_sync_epi();  // every thread's row holds its final sums
-    const int q0 = mti * s.a_step;
-#pragma unroll 1
-    for (int item = row; item < BN * (kUBM / 16); item += kUBM) {
-      const int col = item % BN, g16 = (item / BN) * 16;  // lanes: consecutive columns
-      const int q = q0 + g16, n = nti * s.b_step + col;
-      if (q >= s.M || n >= s.N) continue;  // M = N^2 is a multiple of 16: all 16 rows valid
-      const int p = q / N, r = q - (q / N) * N;
-      const int w = n >> 1, c = n & 1;
-      const long long off = (long long)w * wstride + (long long)p * ld + c * N + r;
-      uint32_t h[8], l[8], m[8];
-#pragma unroll
-      for (int k = 0; k < 16; k += 2) {
-        float x[2];
-        bf16 a[2], b[2], d[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          x[u] = rows[(g16 + k + u) * (BN + 1) + col];
-          a[u] = __float2bfloat16_rn(x[u]);
-          float rr = x[u] - __bfloat162float(a[u]);
-          b[u] = __float2bfloat16_rn(rr);
-          rr -= __bfloat162float(b[u]);
-          d[u] = __float2bfloat16_rn(rr);
-        }
-        h[k / 2] = (uint32_t)__bfloat16_as_ushort(a[0]) | ((uint32_t)__bfloat16_as_ushort(a[1]) << 16);
-        l[k / 2] = (uint32_t)__bfloat16_as_ushort(b[0]) | ((uint32_t)__bfloat16_as_ushort(b[1]) << 16);
-        m[k / 2] = (uint32_t)__bfloat16_as_ushort(d[0]) | ((uint32_t)__bfloat16_as_ushort(d[1]) << 16);
-      }
-      uint4* d0 = reinterpret_cast<uint4*>(vp[0] + off);
-      uint4* d1 = reinterpret_cast<uint4*>(vp[1] + off);
-      d0[0] = make_uint4(h[0], h[1], h[2], h[3]);
-      d0[1] = make_uint4(h[4], h[5], h[6], h[7]);
-      d1[0] = make_uint4(l[0], l[1], l[2], l[3]);
-      d1[1] = make_uint4(l[4], l[5], l[6], l[7]);
-      if (npc > 2) {
-        uint4* d2 = reinterpret_cast<uint4*>(vp[2] + off);
-        d2[0] = make_uint4(m[0], m[1], m[2], m[3]);
-        d2[1] = make_uint4(m[4], m[5], m[6], m[7]);
-      }
-    }
-    named_sync_epi();  // the rows are reused by the next tile's chunk sums
   }
 };
 
