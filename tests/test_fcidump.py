@@ -185,3 +185,34 @@ def test_launch_script_setup(tmp_path):
             launch_script.read_options(bad)
     with pytest.raises(ValueError):
         launch_script.run_afqmc(dict(meta["driver_options"]), nproc=2, tmpdir=d)
+
+
+def test_reader_follows_continuation_blocks(tmp_path):
+    """A dataset whose layout message sits in a continuation block (what the
+    HDF5 library writes once an object header overflows) reads back the same."""
+    fn = str(tmp_path / "x.h5")
+    arr = np.arange(12, dtype=np.float64).reshape(3, 4)
+    fcidump.write_hdf5_datasets(fn, {"a": arr})
+    raw = bytearray(open(fn, "rb").read())
+    u = lambda o, n: int.from_bytes(raw[o:o + n], "little")  # noqa: E731
+    heap, btree = u(88, 8), u(80, 8)
+    snod = u(btree + 32, 8)
+    oh = u(snod + 8 + 8, 8)  # object header of the only dataset
+    # find the layout message (type 8) in the header's message block
+    p, end = oh + 16, oh + 16 + u(oh + 8, 4)
+    while p < end and u(p, 2) != 8:
+        p += 8 + u(p + 2, 2)
+    assert p < end
+    size = u(p + 2, 2)
+    layout_msg = bytes(raw[p:p + 8 + size])
+    # append a continuation block holding the layout message (plus a NIL message)
+    cont_addr = len(raw)
+    block = layout_msg + struct.pack("<HHB3x", 0, 8, 0) + bytes(8)
+    raw += block
+    # replace the layout message in place by a continuation message of the same size
+    cont = struct.pack("<QQ", cont_addr, len(block)) + bytes(size - 16)
+    raw[p:p + 8 + size] = struct.pack("<HHB3x", 0x10, size, 0) + cont
+    raw[oh + 2:oh + 4] = struct.pack("<H", u(oh + 2, 2) + 2)  # the block adds layout + NIL
+    open(fn, "wb").write(bytes(raw))
+    got = fcidump.read_hdf5_datasets(fn)["a"]
+    assert got.dtype == arr.dtype and got.shape == arr.shape and np.array_equal(got, arr)
