@@ -78,8 +78,13 @@ def test_mixed_measurements(case, precision):
     assert err_e / scale < TOL[precision], (err_e, scale)
 
 
+# two and three 128-row M tiles in the propagator (N = 200, N = 300 with UHF 60/58)
+STEP_CASES = CASES[:3] + [(200, (40, 40), 1000, "rhf", "restricted", 4),
+                          (300, (60, 58), 1500, "uhf", "unrestricted", 2)]
+
+
 @pytest.mark.parametrize("precision", ["mixed", "mixed_hi"])
-@pytest.mark.parametrize("case", CASES[:3])
+@pytest.mark.parametrize("case", STEP_CASES)
 def test_mixed_step(case, precision):
     norb, nelec, nchol, tr, wt, W = case
     sys_ = make_system(norb, nelec, nchol, seed=12, trial=tr, chol_scale=0.25)
