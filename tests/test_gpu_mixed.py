@@ -108,15 +108,17 @@ def test_mixed_step(case, precision):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "mixed_hi"])
-def test_mixed_block_energy_error(precision):
-    """Block energies of the mixed path vs the FP64 oracle (same fields)."""
+@pytest.mark.parametrize("shape", [(64, (16, 16), 300, 32, 5, 3), (200, (40, 40), 1000, 16, 3, 2)])
+def test_mixed_block_energy_error(precision, shape):
+    """Block energies of the mixed path vs the FP64 oracle (same fields), at
+    N = 64 and at the headline orbital count N = 200."""
     from ad_afqmc_b200 import sampling
 
-    sys_ = make_system(64, (16, 16), 300, seed=13, trial="rhf", chol_scale=0.25)
-    W, S, nb = 32, 5, 3
+    norb, nelec, nchol, W, S, nb = shape
+    sys_ = make_system(norb, nelec, nchol, seed=13, trial="rhf", chol_scale=0.25)
     walkers = _walkers(sys_, W, 6, "restricted")
     rng = np.random.default_rng(7)
-    fields = [rng.standard_normal((S, W, 300)) for _ in range(nb)]
+    fields = [rng.standard_normal((S, W, nchol)) for _ in range(nb)]
     uni = list(rng.random(nb))
     o_trial, o_ham, o_wave, o_prop = oracle_system(sys_, "restricted", 0.005)
     o_prop.n_walkers = W
