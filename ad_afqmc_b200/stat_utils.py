@@ -26,6 +26,8 @@ def blocking_analysis(weights, energies, neql=0, printQ=False, writeBlockedQ=Fal
         mean = (bw * be).sum() / v1
         err = ((bw * (be - mean) ** 2).sum() / (v1 - v2 / v1) / (nb - 1)) ** 0.5
         errors.append(err)
+        if writeBlockedQ:
+            np.savetxt(f"samples_blocked_{i}.dat", np.stack((bw, be)).T)
         if printQ:
             print(f"  {i:5d}           {nb:6d}       {mean:.8e}       {err:.6e}")
         if err < 1.05 * prev and plateau is None:
