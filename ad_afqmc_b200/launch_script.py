@@ -101,14 +101,16 @@ def set_trial(options: Dict, mo_coeff, norb: int, nelec_sp: Tuple[int, int]):
            np.ascontiguousarray(mo_coeff[1][:, :nelec_sp[1]])]
     wave_data = {"rdm1": np.array([m @ m.T for m in mos])}
     if options.get("prjlo") is not None:
-        trial = wavefunctions.rhf_lno(norb, nelec_sp)
+        trial = wavefunctions.rhf_lno(norb, nelec_sp, n_chunks=options["n_chunks"])
         wave_data["mo_coeff"] = mos[0]
         wave_data["prjlo"] = np.asarray(options["prjlo"], dtype=np.float64)
     elif options["trial"] == "rhf":
-        trial = wavefunctions.rhf(norb, nelec_sp)
+        trial = wavefunctions.rhf(norb, nelec_sp, n_chunks=options["n_chunks"],
+                                  projector=options.get("symmetry_projector"))
         wave_data["mo_coeff"] = mos[0]
     else:
-        trial = wavefunctions.uhf(norb, nelec_sp)
+        trial = wavefunctions.uhf(norb, nelec_sp, n_chunks=options["n_chunks"],
+                                  projector=options.get("symmetry_projector"))
         wave_data["mo_coeff"] = mos
     return trial, wave_data
 

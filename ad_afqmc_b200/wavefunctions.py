@@ -35,14 +35,14 @@ def _ptrs(walkers):
     return _lib.pair(walkers.data.data_ptr(), None)
 
 
-@dataclass
 class wave_function:
-    """Base class (wavefunctions.py:19-493) restricted to the single-determinant trials."""
+    """Base class (wavefunctions.py:19-493) restricted to the single-determinant
+    trials.  As in the reference it is not a dataclass itself: each trial class
+    declares its own fields, so their order is the reference's."""
 
     norb: int
     nelec: Tuple[int, int]
     n_chunks: int = 1
-    projector: Optional[str] = None
 
     # -- trial orbitals on the device, cached in wave_data -------------------
     def _mo_list(self, wave_data: dict) -> List[torch.Tensor]:
@@ -156,7 +156,8 @@ class wave_function:
         return wave_data
 
     def __hash__(self) -> int:
-        return hash((type(self).__name__, self.norb, tuple(self.nelec)))
+        """wavefunctions.py:492-493."""
+        return hash(tuple(self.__dict__.values()))
 
 
 def _sym(h1: torch.Tensor) -> torch.Tensor:
@@ -168,12 +169,21 @@ def _sym(h1: torch.Tensor) -> torch.Tensor:
 
 @dataclass
 class rhf(wave_function):
-    """Restricted Hartree-Fock trial (wavefunctions.py:1038-1235)."""
+    """Restricted Hartree-Fock trial (wavefunctions.py:1038-1235).  Fields in the
+    reference's order (:1053-1057): norb, nelec, n_opt_iter, n_chunks, projector."""
 
+    norb: int
+    nelec: Tuple[int, int]
     n_opt_iter: int = 30
+    n_chunks: int = 1
+    projector: Optional[str] = None
 
     def __post_init__(self):
         assert self.nelec[0] == self.nelec[1], "RHF requires equal number of up and down electrons."
+
+    def __hash__(self) -> int:
+        """wavefunctions.py:1234-1235."""
+        return hash(tuple(self.__dict__.values()))
 
     def _calc_rdm1(self, wave_data: dict) -> torch.Tensor:
         mo = to_dev(wave_data["mo_coeff"])
@@ -194,11 +204,14 @@ class rhf(wave_function):
 
 
 @dataclass
-
 class rhf_lno(rhf):
     """RHF trial of an LNO fragment (wavefunctions.py:6871-6926): the rhf
     measurements plus the orbital energy of the fragment's localized orbital,
     whose projector is wave_data["prjlo"] ((n_lo, nocc), lnoafqmc.py:147)."""
+
+    def __hash__(self) -> int:
+        """wavefunctions.py:6925-6926."""
+        return hash(tuple(self.__dict__.values()))
 
     def calc_orbenergy(self, walkers: walker_batch, ham_data: dict, wave_data: dict, *,
                        engine=None) -> torch.Tensor:
@@ -217,10 +230,21 @@ class rhf_lno(rhf):
         )
         return out
 
-class uhf(wave_function):
-    """Unrestricted Hartree-Fock trial (wavefunctions.py:1238-1499)."""
 
+@dataclass
+class uhf(wave_function):
+    """Unrestricted Hartree-Fock trial (wavefunctions.py:1238-1499).  Fields in the
+    reference's order (:1251-1255): norb, nelec, n_opt_iter, n_chunks, projector."""
+
+    norb: int
+    nelec: Tuple[int, int]
     n_opt_iter: int = 30
+    n_chunks: int = 1
+    projector: Optional[str] = None
+
+    def __hash__(self) -> int:
+        """wavefunctions.py:1498-1499."""
+        return hash(tuple(self.__dict__.values()))
 
     def _calc_rdm1(self, wave_data: dict) -> torch.Tensor:
         m0, m1 = to_dev(wave_data["mo_coeff"][0]), to_dev(wave_data["mo_coeff"][1])
