@@ -149,6 +149,24 @@ class Engine:
             self.work = new
         self.work_bytes = self.work.numel() * 8
 
+    def check_status(self) -> None:
+        """Raise AfqError if a bounded device-side wait of the tensor-core
+        kernels ran out on this workspace since the last check (the flag is
+        read and cleared by afq_check_status, which synchronizes the stream)."""
+        _lib.check(_lib.lib().afq_check_status(C.byref(self.dims), self.work.data_ptr(), self.work_bytes,
+                                               _lib.stream_handle()), "device status")
+
+    def status_flag(self) -> torch.Tensor:
+        """(1,) int32 view of this workspace's device error flag (0 = clear),
+        for code that copies it out inside a CUDA graph (afq_status_flag).
+        The view follows the current workspace: take it again after
+        ensure_workspace."""
+        p = C.c_void_p()
+        _lib.check(_lib.lib().afq_status_flag(C.byref(self.dims), self.work.data_ptr(), self.work_bytes,
+                                              C.byref(p)), "afq_status_flag")
+        off = (int(p.value) - self.work.data_ptr()) // 4
+        return self.work.view(torch.int32)[off:off + 1]
+
     @property
     def handle(self) -> Tuple[int, int, int]:
         return self.prepared.data_ptr(), self.work.data_ptr(), self.work_bytes

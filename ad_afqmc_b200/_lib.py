@@ -16,6 +16,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "lib", "libafqmc_b200.so")
 
 AFQ_OK = 0
+AFQ_ERR_TIMEOUT = 8
 AFQ_RESTRICTED, AFQ_UNRESTRICTED = 0, 1
 AFQ_TRIAL_RHF, AFQ_TRIAL_UHF = 0, 1
 AFQ_FP64, AFQ_MIXED, AFQ_MIXED_HI = 0, 1, 2
@@ -134,6 +135,10 @@ _SIGS = {
                                 C.c_void_p], C.c_int),
     "afq_set_tuning": ([C.POINTER(afq_dims), C.c_void_p], C.c_int),
     "afq_get_tuning": ([C.POINTER(afq_dims), C.POINTER(afq_tuning)], C.c_int),
+    "afq_check_status": ([C.POINTER(afq_dims), C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_status_flag": ([C.POINTER(afq_dims), C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
+    "afq_test_wait_timeout": ([C.POINTER(afq_dims), C.c_void_p, C.c_size_t, C.c_uint32, C.c_void_p],
+                              C.c_int),
     "afq_launch_count": ([C.c_int, C.POINTER(C.c_ulonglong)], C.c_int),
     "afq_profile_begin": ([C.c_int], C.c_int),
     "afq_profile_end": ([C.POINTER(C.c_double), C.POINTER(C.c_int)], C.c_int),

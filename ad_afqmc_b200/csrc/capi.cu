@@ -137,6 +137,7 @@ const char* afq_status_string(int status) {
     case AFQ_ERR_ALIGN: return "pointer not 16-byte aligned";
     case AFQ_ERR_ARG: return "argument out of range";
     case AFQ_ERR_LIMIT: return "size exceeds the fixed static scratch capacity";
+    case AFQ_ERR_TIMEOUT: return "a device-side wait timed out; results since the last check are invalid";
     default: return "unknown status";
   }
 }

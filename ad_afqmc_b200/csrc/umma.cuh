@@ -55,8 +55,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // Bounded wait: ~1e8 polls (each try_wait already suspends for a while).
 constexpr uint32_t kMaxPolls = 1u << 27;
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kMaxPolls; ++i)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          uint32_t max_polls = kMaxPolls) {
+  for (uint32_t i = 0; i < max_polls; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

@@ -11,6 +11,7 @@ per-block scalars, as in stat_utils.py.
 
 from __future__ import annotations
 
+import warnings
 from typing import Optional, Tuple
 
 import numpy as np
@@ -31,6 +32,17 @@ def _run_equilibration(ham, ham_data, prop, prop_data, trial, wave_data, sampler
             prop_data["weights"], zeta)
         prop_data["e_estimate"] = 0.9 * prop_data["e_estimate"] + 0.1 * e
     return prop_data
+
+
+def _warn_nonfinite(e: np.ndarray, w: np.ndarray) -> None:
+    """Block energies or weights that are not finite (a population whose
+    weights all went to zero gives 0/0) pass through the analysis as in the
+    reference; say so instead of failing silently."""
+    bad = ~(np.isfinite(e) & np.isfinite(w))
+    if bad.any():
+        warnings.warn(f"{int(bad.sum())} of {len(e)} blocks have non-finite energy or weight "
+                      f"(first at block {int(np.argmax(bad))}); the population may have collapsed",
+                      RuntimeWarning, stacklevel=3)
 
 
 def afqmc_blocks(ham, ham_data, prop, prop_data, trial, wave_data, smp, n_blocks,
@@ -69,6 +81,7 @@ def afqmc_energy(ham_data: dict, ham, propagator, trial, wave_data: dict, sample
                                                 sampler, sampler.n_blocks)
     e = energies.cpu().numpy()
     w = weights.cpu().numpy()
+    _warn_nonfinite(e, w)
     np.savetxt(tmpdir + "/samples_raw.dat", np.stack((w, e)).T)
     clean, _ = stat_utils.reject_outliers(np.stack((w, e)).T, 1)
     return stat_utils.blocking_analysis(clean[:, 0], clean[:, 1], neql=0)
@@ -118,6 +131,7 @@ def afqmc_LNOenergy(ham_data: dict, ham, propagator, trial, wave_data: dict, sam
     w = np.array(weights[: truncate_at + 1])
     e = np.array(energies[: truncate_at + 1])
     o = np.array(orbes[: truncate_at + 1])
+    _warn_nonfinite(e, w)
     np.savetxt(tmpdir + "/samples_raw.dat", np.stack((w, e)).T)
     clean, _ = stat_utils.reject_outliers(np.stack((w, e)).T, 1)
     e_afqmc, e_err = stat_utils.blocking_analysis(clean[:, 0], clean[:, 1], neql=0)

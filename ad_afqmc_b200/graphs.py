@@ -78,6 +78,8 @@ class BlockGraph:
                 -1, trial.nelec[0]).contiguous()
             self.e_buf = torch.empty(W, dtype=torch.complex128, device=dev)
             self.o_buf = torch.empty(W, dtype=torch.complex128, device=dev)
+        # device error flags of the recorded blocks, OR-ed over replays until check_status()
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.w_tmp = torch.empty_like(prop_data["weights"])
         self.idx = torch.empty(W, dtype=torch.int32, device=dev)
         self.small = torch.empty(W * 16, dtype=torch.float64, device=dev)  # own: solves may overlap
@@ -112,6 +114,7 @@ class BlockGraph:
             sc[2].div_(self.prop.n_walkers)
             if self.update_estimate:
                 sc[0].mul_(0.9).add_(0.1 * self.block_out[0])
+            self._fold_status()
             self.launches_per_block = _lib.launch_count() - n0
             pd.pop("_afq_green_of", None)
             return
@@ -132,8 +135,23 @@ class BlockGraph:
         sc[2].div_(self.prop.n_walkers)
         if self.update_estimate:
             sc[0].mul_(0.9).add_(0.1 * self.block_out[0])
+        self._fold_status()
         self.launches_per_block = _lib.launch_count() - n0
         pd.pop("_afq_green_of", None)
+
+    def _fold_status(self) -> None:
+        """Move the engine's device error flag into self.status (device ops
+        only, so it records into the graph)."""
+        flag = self.eng.status_flag()
+        torch.maximum(self.status, flag, out=self.status)
+        flag.zero_()
+
+    def check_status(self) -> None:
+        """Raise AfqError if a device-side wait timed out in any block since
+        the last check; reads (and clears) the recorded flag."""
+        if int(self.status.item()) != 0:
+            self.status.zero_()
+            raise _lib.AfqError("a device-side wait timed out: the blocks since the last check are invalid")
 
     def _lno_block_end(self, lib, stream) -> None:
         """sampler_lno._block_scan after the steps (sampling.py:586-631): QR,
@@ -267,6 +285,7 @@ class HostFieldBlocks:
         self.uploaded = -1  # last block whose fields were queued
         W = bg.prop.n_walkers
         self.out_host = torch.empty(2 + W, dtype=torch.float64).pin_memory()
+        self.status_host = torch.zeros(1, dtype=torch.int32).pin_memory()
         self.h2d_bytes = bg.fields.numel() * bg.fields.element_size()
         self.d2h_bytes = self.out_host.numel() * self.out_host.element_size()
 
@@ -302,7 +321,11 @@ class HostFieldBlocks:
             self._upload(self.n + 1, next_host_fields)
         self.out_host[:2].copy_(self.bg.block_out[:2], non_blocking=True)
         self.out_host[2:].copy_(self.bg.pd["weights"], non_blocking=True)
+        self.status_host.copy_(self.bg.status, non_blocking=True)
         cur.synchronize()
         self.n += 1
+        if int(self.status_host[0]) != 0:
+            self.bg.status.zero_()
+            raise _lib.AfqError(f"block {self.n - 1}: a device-side wait timed out; its results are invalid")
         return self.out_host.numpy().copy()
 

@@ -89,6 +89,7 @@ class sampler:
         sc[2].div_(nb * prop.n_walkers)
         be, bw = out[:, 0], out[:, 1]
         prop_data["block_energies"] = out
+        eng.check_status()  # a timed-out device wait invalidates these blocks
         return torch.sum(be * bw) / torch.sum(bw), prop_data
 
     def propagate_free(self, ham, ham_data: dict, prop, prop_data: dict, trial, wave_data: dict):
@@ -195,4 +196,5 @@ class sampler_lno(sampler):
         sc[2].div_(nb * prop.n_walkers)
         be, bw, bo = out[:, 0], out[:, 1], out[:, 2]
         prop_data["block_energies"] = out
+        eng.check_status()
         return torch.sum(be * bw) / torch.sum(bw), prop_data, torch.sum(bo * bw) / torch.sum(bw)

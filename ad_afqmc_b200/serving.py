@@ -168,14 +168,17 @@ class Solve:
 
 
 class Server:
-    def __init__(self, precision: str = "mixed", hbm_budget_gb: float = 170.0, max_slots: int = 16,
+    def __init__(self, precision: str = "mixed", hbm_budget_gb: float = 180.0, max_slots: int = 16,
                  n_prop_steps: int = 10, n_eql: int = 5, target_error: float = 5e-4,
                  max_blocks: int = 40, stop_rule: str = "sem", min_blocks: int = 5,
                  setup_thread: bool = True, reserve_gb_per_slot: float = 4.0):
         if stop_rule not in ("sem", "blocking"):
             raise ValueError(f"stop_rule must be 'sem' or 'blocking', not {stop_rule!r}")
         self.precision = precision
-        self.budget = int(hbm_budget_gb * 1e9)
+        # the requested budget, capped by what the device has free now (less 2 GB of headroom
+        # for the CUDA context, cuBLAS workspaces and allocator rounding)
+        free = torch.cuda.mem_get_info()[0] if torch.cuda.is_available() else int(hbm_budget_gb * 1e9)
+        self.budget = int(min(hbm_budget_gb * 1e9, free - 2e9))
         self.max_slots = max_slots
         self.S = n_prop_steps
         self.n_eql = n_eql
@@ -345,6 +348,36 @@ def summarize(results: List[Result], wall: float) -> Dict:
             "mean_blocks": float(np.mean([r.n_blocks for r in results]))}
 
 
+def bench(rate: float = 20.0, duration: float = 10.0, precision: str = "mixed", slots: int = 16,
+          max_blocks: int = 40, stop_rule: str = "sem", lno: bool = False, baseline: bool = True) -> Dict:
+    """The serving workload: Poisson arrivals at ``rate``/s for ``duration``
+    s, served with continuous batching, then (``baseline``) the same requests
+    solved one by one in arrival order.  Returns latency percentiles and
+    fragments/s of both."""
+    reqs = make_requests(rate, duration, lno=lno)
+    srv = Server(precision, max_slots=slots, max_blocks=max_blocks, stop_rule=stop_rule)
+    # warm the CUDA context and kernels with throw-away requests of every path
+    warm = make_requests(4.0, 1.0, seed=7, lno=lno)[:3]
+    srv.run(warm, realtime=False)
+    one_by_one(warm[:1], srv)
+    t0 = time.perf_counter()
+    res = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    out = {"workload": (f"Poisson {rate}/s for {duration} s: N~U[30,160], No=round(N/4), G~U[4N,6N], "
+                        f"W~U[64,256], 10% N=250/G=1250; stop std err < 0.5 mHa ({stop_rule}) "
+                        f"or {max_blocks} blocks after 5 equilibration blocks"),
+           "construction": ("synthetic recipe with the Cholesky vectors scaled by 0.035*sqrt(100/N) "
+                            "(the unscaled recipe's block-energy noise keeps most fragments from "
+                            "reaching 0.5 mHa); the work per block does not depend on the scale"),
+           "precision": precision, "slots": slots, "lno": lno, "hbm_budget_gb": srv.budget / 1e9,
+           "serving": summarize(res, wall)}
+    if baseline:
+        t0 = time.perf_counter()
+        base = one_by_one(reqs, srv)
+        out["one_by_one"] = summarize(base, time.perf_counter() - t0)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--rate", type=float, default=20.0)
@@ -358,24 +391,8 @@ def main():
                     help="LNO fragments: orbital energies (rhf_lno), stop on their standard error")
     a = ap.parse_args()
     torch.cuda.set_device(0)
-    reqs = make_requests(a.rate, a.duration, lno=a.lno)
-    srv = Server(a.precision, max_slots=a.slots, max_blocks=a.max_blocks, stop_rule=a.stop_rule)
-    # warm the CUDA context and kernels with throw-away requests of every path
-    warm = make_requests(4.0, 1.0, seed=7, lno=a.lno)[:3]
-    srv.run(warm, realtime=False)
-    one_by_one(warm[:1], srv)
-    t0 = time.perf_counter()
-    res = srv.run(reqs)
-    wall = time.perf_counter() - t0
-    out = {"workload": (f"Poisson {a.rate}/s for {a.duration} s: N~U[30,160], No=round(N/4), G~U[4N,6N], "
-                        f"W~U[64,256], 10% N=250/G=1250; stop std err < 0.5 mHa ({a.stop_rule}) "
-                        f"or {a.max_blocks} blocks after 5 equilibration blocks"),
-           "precision": a.precision, "slots": a.slots, "lno": a.lno, "serving": summarize(res, wall)}
-    if not a.no_baseline:
-        t0 = time.perf_counter()
-        base = one_by_one(reqs, srv)
-        out["one_by_one"] = summarize(base, time.perf_counter() - t0)
-    print(json.dumps(out))
+    print(json.dumps(bench(a.rate, a.duration, a.precision, a.slots, a.max_blocks, a.stop_rule, a.lno,
+                           baseline=not a.no_baseline)))
 
 
 if __name__ == "__main__":

@@ -42,7 +42,8 @@ typedef enum afq_status {
   AFQ_ERR_WORKSPACE = 4,  /* prepared/workspace buffer too small          */
   AFQ_ERR_ALIGN = 5,      /* a pointer is not 16-byte aligned             */
   AFQ_ERR_ARG = 6,        /* an enum/flag argument is out of range        */
-  AFQ_ERR_LIMIT = 7       /* size beyond a fixed (static) scratch capacity */
+  AFQ_ERR_LIMIT = 7,      /* size beyond a fixed (static) scratch capacity */
+  AFQ_ERR_TIMEOUT = 8     /* a bounded device-side wait ran out (afq_check_status) */
 } afq_status;
 
 enum { AFQ_RESTRICTED = 0, AFQ_UNRESTRICTED = 1 };      /* walker_type  */
@@ -296,6 +297,25 @@ typedef struct afq_tuning {
 
 int afq_set_tuning(const afq_dims* d, const afq_tuning* t);
 int afq_get_tuning(const afq_dims* d, afq_tuning* out);
+
+/* Device-side failure status of a workspace (no counterpart in the reference,
+ * whose XLA kernels have no waits of their own; its only guards are the
+ * numerical masks of propagation.py:321-331 and the driver's check of the
+ * initial overlaps, driver.py:76-79).  The tensor-core kernels bound every
+ * mbarrier wait; a wait that runs out sets a flag in the workspace, unwinds
+ * and returns, after the launching call already returned AFQ_OK, so that
+ * call's walkers or energies are invalid.  afq_check_status synchronizes
+ * `stream`, reads the flag, clears it and returns AFQ_ERR_TIMEOUT if it was
+ * set (call it once per block: the flag stays set until read).
+ * afq_status_flag returns the flag's device address (an int32, 0 = clear) for
+ * code that copies it out inside a CUDA graph instead.  afq_test_wait_timeout
+ * is a test hook: one thread waits on an mbarrier that nothing arrives at,
+ * with the GEMMs' bounded poll loop limited to `polls` (1..4096), and sets the
+ * flag when the wait runs out; no copy or MMA is in flight, so nothing faults. */
+int afq_check_status(const afq_dims* d, void* work, size_t work_bytes, void* stream);
+int afq_status_flag(const afq_dims* d, void* work, size_t work_bytes, int32_t** flag);
+int afq_test_wait_timeout(const afq_dims* d, void* work, size_t work_bytes, uint32_t polls,
+                          void* stream);
 
 /* Instrumentation (no counterpart in the reference, which has no native
  * code): launches of one kernel family (kernel_id >= 0) or of all library

@@ -104,3 +104,25 @@ def test_run_afqmc_driver_options(calc_dir, precision):
     assert abs(e - e_ref) < max(0.01, 5.0 * err), (e, err, e_ref)
     assert e < e_uhf - 0.05
     assert os.path.isfile(os.path.join(d, "samples_raw.dat"))
+
+
+def test_run_afqmc_tight_statistics(calc_dir):
+    """The driver test's energy to a standard error below 0.3 mHa (1000
+    walkers, 25 blocks of 10 x 50 steps), compared with both energies the
+    reference asserts (tests/test_driver.py:19-33 with two ranks of 50
+    walkers, :74-86 with one) at three combined standard errors.  Each
+    reference value is one run of its own random stream, so its own
+    statistical error counts: it is the standard error this driver gives at
+    the reference's settings (and that over sqrt(2) for the two-rank run)."""
+    d, e_uhf, meta = calc_dir
+    base = dict(meta["driver_options"], precision="fp64")
+    _, err_ref = launch_script.run_afqmc(dict(base), tmpdir=d)
+    err_ref = float(err_ref) if err_ref is not None and np.isfinite(err_ref) else 2e-3
+    e, err = launch_script.run_afqmc(dict(base, n_walkers=1000, n_blocks=25), tmpdir=d)
+    assert err is not None and np.isfinite(err)
+    print(f"run_afqmc 1000 walkers: E = {e:.6f} +- {err:.6f} Ha (reference settings: +- {err_ref:.6f})")
+    assert err < 3e-4
+    refs = [(meta["reference_values"]["afqmc_energy_1proc"][0], err_ref),
+            (meta["reference_values"]["afqmc_energy_2proc"][0], err_ref / np.sqrt(2.0))]
+    for e_ref, s_ref in refs:
+        assert abs(e - e_ref) < 3.0 * np.hypot(err, s_ref), (e, err, e_ref, s_ref)

@@ -39,6 +39,7 @@ def _dev(w):
 
 
 CASES = [
+    (10, (5, 5), 50, "rhf", "restricted", 16),  # the N = 10 workload's shape
     (24, (6, 6), 96, "rhf", "restricted", 16),
     (64, (16, 16), 300, "rhf", "restricted", 40),
     (48, (13, 11), 200, "uhf", "unrestricted", 24),
@@ -79,7 +80,7 @@ def test_mixed_measurements(case, precision):
 
 
 # two and three 128-row M tiles in the propagator (N = 200, N = 300 with UHF 60/58)
-STEP_CASES = CASES[:3] + [(200, (40, 40), 1000, "rhf", "restricted", 4),
+STEP_CASES = CASES[:4] + [(200, (40, 40), 1000, "rhf", "restricted", 4),
                           (300, (60, 58), 1500, "uhf", "unrestricted", 2)]
 
 
@@ -107,26 +108,53 @@ def test_mixed_step(case, precision):
     assert np.allclose(_np(d_pd["weights"]), o_pd["weights"], rtol=10 * TOL[precision], atol=1e-6)
 
 
+BLOCK_SHAPES = [
+    # norb, nelec, nchol, trial, walkers, steps per block, blocks, Cholesky scale
+    (64, (16, 16), 300, "rhf", 32, 5, 3, 0.25),
+    (200, (40, 40), 1000, "rhf", 16, 3, 2, 0.1),
+    # the N = 300 UHF workload's shape (Na/Nb = 60/58, G = 1500)
+    (300, (60, 58), 1500, "uhf", 4, 2, 1, 0.1),
+]
+
+
 @pytest.mark.parametrize("precision", ["mixed", "mixed_hi"])
-@pytest.mark.parametrize("shape", [(64, (16, 16), 300, 32, 5, 3), (200, (40, 40), 1000, 16, 3, 2)])
+@pytest.mark.parametrize("shape", BLOCK_SHAPES)
 def test_mixed_block_energy_error(precision, shape):
-    """Block energies of the mixed path vs the FP64 oracle (same fields), at
-    N = 64 and at the headline orbital count N = 200."""
+    """Block energies of the mixed path vs the FP64 oracle (same walkers,
+    fields and uniforms), within 0.1 mHa, in the unclamped regime: at most 1 %
+    of the final local energies lie further than sqrt(2/dt) from e_estimate
+    (the clamp of sampling.py:84-88 would otherwise replace them by
+    e_estimate and make the block energies agree by construction).  The
+    unclamped weighted local energy of the final walkers (FP64 evaluation of
+    the mixed-propagated walkers vs the oracle's) is bounded the same way."""
     from ad_afqmc_b200 import sampling
 
-    norb, nelec, nchol, W, S, nb = shape
-    sys_ = make_system(norb, nelec, nchol, seed=13, trial="rhf", chol_scale=0.25)
-    walkers = _walkers(sys_, W, 6, "restricted")
+    norb, nelec, nchol, tr, W, S, nb, scale = shape
+    wt = "restricted" if tr == "rhf" else "unrestricted"
+    sys_ = make_system(norb, nelec, nchol, seed=13, trial=tr, chol_scale=scale)
+    walkers = _walkers(sys_, W, 6, wt)
     rng = np.random.default_rng(7)
     fields = [rng.standard_normal((S, W, nchol)) for _ in range(nb)]
     uni = list(rng.random(nb))
-    o_trial, o_ham, o_wave, o_prop = oracle_system(sys_, "restricted", 0.005)
+    dt = 0.005
+    o_trial, o_ham, o_wave, o_prop = oracle_system(sys_, wt, dt)
     o_prop.n_walkers = W
     o_pd = o_prop.init_prop_data(o_trial, o_wave, o_ham, init_walkers=copy.deepcopy(walkers))
     e_o, o_pd = orc.Sampler(S, nb, 1).propagate_phaseless(o_prop, o_trial, o_ham, o_pd, o_wave,
                                                           ListSource(fields, uni))
-    d_trial, d_ham, d_wave, d_prop, ham = device_system(sys_, "restricted", 0.005, W, precision=precision)
+    d_trial, d_ham, d_wave, d_prop, ham = device_system(sys_, wt, dt, W, precision=precision)
     d_pd = d_prop.init_prop_data(d_trial, d_wave, d_ham, 0, init_walkers=_dev(walkers))
     e_d, d_pd = sampling.sampler(S, nb, 1, field_source=ListSource(fields, uni)).propagate_phaseless(
         ham, d_ham, d_prop, d_pd, d_trial, d_wave)
+    # regime: local energies of the final walkers against e_estimate
+    el_o = np.real(o_trial.calc_energy(orc.orthonormalize(o_pd["walkers"]), o_ham, o_wave))
+    clamped = float(np.mean(np.abs(el_o - o_pd["e_estimate"]) > (2.0 / dt) ** 0.5))
+    assert clamped <= 0.01, clamped
+    assert o_pd["n_killed_walkers"] == 0
     assert abs(float(e_d) - e_o) < 1e-4  # 0.1 mHa
+    # unclamped weighted local energy of the final walkers, both evaluated in FP64
+    el_d = _np(torch.real(d_trial.calc_energy(d_pd["walkers"].orthonormalize(), d_ham, d_wave)))
+    w_d, w_o = _np(d_pd["weights"]), o_pd["weights"]
+    e_unc_d = float(np.sum(el_d * w_d) / np.sum(w_d))
+    e_unc_o = float(np.sum(el_o * w_o) / np.sum(w_o))
+    assert abs(e_unc_d - e_unc_o) < 1e-4, (e_unc_d, e_unc_o)

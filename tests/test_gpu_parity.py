@@ -304,3 +304,34 @@ def test_config_uhf_n300_subset_parity():
     for s in range(2):
         assert rel_err(_np(d_pd["walkers"].data[s]), o_pd["walkers"][s]) < 1e-10
     assert np.allclose(_np(d_pd["weights"]), o_pd["weights"], rtol=1e-10, atol=1e-13)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_config_rhf_n200_full_tile_step(precision):
+    """A full tile of walkers at the N = 200 / G = 1000 headline shape (128
+    walkers: whole 128-column tiles in the force-bias and VHS GEMMs and 16 row
+    tiles of the exchange): one phaseless step and the local energies of every
+    walker against the oracle, FP64 to 1e-10 and BF16x3 to 1e-4 relative."""
+    from ad_afqmc_b200.walkers import RHFWalkers
+
+    sys_ = make_system(200, (40, 40), 1000, seed=1002, trial="rhf", chol_scale=0.1)
+    rng = np.random.default_rng(31)
+    W = 128
+    walkers = near_trial_walkers(rng, sys_.mo_coeff, W, eps=0.05)
+    fields = rng.standard_normal((W, 1000))
+    o_trial, o_ham, o_wave, o_prop = oracle_system(sys_, "restricted", 0.005)
+    o_prop.n_walkers = W
+    o_pd = o_prop.init_prop_data(o_trial, o_wave, o_ham, init_walkers=walkers.copy())
+    o_pd = o_prop.propagate_constrained(o_trial, o_ham, o_pd, fields, o_wave)
+    d_trial, d_ham, d_wave, d_prop, _ = device_system(sys_, "restricted", 0.005, W, precision=precision)
+    d_pd = d_prop.init_prop_data(d_trial, d_wave, d_ham, 0, init_walkers=RHFWalkers(walkers.copy()))
+    d_pd = d_prop.propagate_constrained(d_trial, d_ham, d_pd, fields, d_wave)
+    tol = 1e-10 if precision == "fp64" else 1e-4
+    dw = _np(d_pd["walkers"].data)
+    for w in range(W):
+        assert rel_err(dw[w], o_pd["walkers"][w]) < tol, w
+    assert np.allclose(_np(d_pd["weights"]), o_pd["weights"], rtol=10 * tol, atol=1e-12)
+    e_o = np.real(o_trial.calc_energy(o_pd["walkers"], o_ham, o_wave))
+    e_d = _np(torch.real(d_trial.calc_energy(d_pd["walkers"], d_ham, d_wave)))
+    # mixed: the walkers differ at the 1e-5 level, which moves E_L (~ -290 Ha) by ~1e-3 Ha
+    assert np.max(np.abs(e_d - e_o)) < (1e-8 if precision == "fp64" else 1e-2)

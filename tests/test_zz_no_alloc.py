@@ -63,6 +63,34 @@ def test_static_overlap_matches_workspace_path_twice(kind):
         assert torch.allclose(got, ref, rtol=1e-12, atol=0), call
 
 
+@pytest.mark.parametrize("kind", ["rhf", "uhf"])
+def test_static_overlap_matches_oracle_at_capacity(kind):
+    """Exactly the capacity (8192 walkers), against the NumPy oracle's
+    determinants, not only against the workspace entry point."""
+    from ad_afqmc_b200 import wavefunctions
+    from ad_afqmc_b200.walkers import RHFWalkers, UHFWalkers
+    from oracle import afqmc_oracle as orc
+
+    rng = np.random.default_rng(23)
+    W, N = STATIC_MAX_WALKERS, 12
+    if kind == "rhf":
+        sys_ = make_system(N, (4, 4), 20, seed=5, trial="rhf")
+        trial, o_trial = wavefunctions.rhf(N, (4, 4)), orc.RHFTrial(N, (4, 4))
+        host = sys_.mo_coeff[None] + 0.3 * (rng.standard_normal((W, N, 4)) + 1j * rng.standard_normal((W, N, 4)))
+        w = RHFWalkers(host.copy())
+    else:
+        sys_ = make_system(N, (5, 3), 20, seed=6, trial="uhf")
+        trial, o_trial = wavefunctions.uhf(N, (5, 3)), orc.UHFTrial(N, (5, 3))
+        host = [m[None] + 0.3 * (rng.standard_normal((W, N, m.shape[1])) + 1j * rng.standard_normal((W, N, m.shape[1])))
+                for m in sys_.mo_coeff]
+        w = UHFWalkers([h.copy() for h in host])
+    wave = sys_.wave_data()
+    ref = o_trial.calc_overlap(host, wave)
+    for _ in range(2):
+        got = _static_overlap(trial, w, wave).cpu().numpy()
+        assert np.allclose(got, ref, rtol=1e-10, atol=0)
+
+
 def test_static_overlap_rejects_too_many_walkers():
     from ad_afqmc_b200 import wavefunctions
     from ad_afqmc_b200.wavefunctions import _ptrs
