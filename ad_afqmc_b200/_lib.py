@@ -135,6 +135,17 @@ _SIGS = {
                                 C.c_void_p], C.c_int),
     "afq_set_tuning": ([C.POINTER(afq_dims), C.c_void_p], C.c_int),
     "afq_get_tuning": ([C.POINTER(afq_dims), C.POINTER(afq_tuning)], C.c_int),
+    "afq_intermediates_workspace_size": ([C.c_int32, C.c_int32, C.POINTER(C.c_size_t)], C.c_int),
+    "afq_measurement_intermediates": ([C.c_int32, C.c_int32 * 2, C.c_int32, C.c_int32, C.c_void_p * 2,
+                                       C.c_void_p, C.c_void_p, C.c_void_p * 2, C.c_void_p * 2, C.c_void_p,
+                                       C.c_size_t, C.c_void_p], C.c_int),
+    "afq_propagation_intermediates": ([C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
+    "afq_expm": ([C.c_int32, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p],
+                 C.c_int),
+    "afq_eigh_desc": ([C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p],
+                      C.c_int),
     "afq_check_status": ([C.POINTER(afq_dims), C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
     "afq_status_flag": ([C.POINTER(afq_dims), C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
     "afq_test_wait_timeout": ([C.POINTER(afq_dims), C.c_void_p, C.c_size_t, C.c_uint32, C.c_void_p],

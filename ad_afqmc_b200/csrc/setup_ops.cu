@@ -1,0 +1,609 @@
+// Per-solve Hamiltonian intermediates on the device (FP64).
+//
+//  measurement   h1[s] <- (h1[s] + h1[s]^T) / 2 ;  rot_h1 = C^T h ;  rot_chol[g] = C^T L_g
+//                (rhf/uhf._build_measurement_intermediates, wavefunctions.py:1215-1232, 1472-1496)
+//  propagation   mf_shifts[g] = i sum(L_g o rho) ;  h0_prop = -h0 - sum(mf^2) / 2 ;
+//                v0 = 1/2 sum_g L_g L_g ;  v1 = sum_g Re(i mf_g) L_g ;
+//                exp_h1 = expm(-dt/2 (h1 - v0 - v1))
+//                (propagator_afqmc._build_propagation_intermediates, propagation.py:378-438)
+//  natural orbitals  eigenpairs of a symmetric matrix, descending
+//                (wave_function.get_init_walkers, wavefunctions.py:427-466)
+//
+// The contractions run on the FP64 tensor cores through the same DMMA main
+// loop as the walker kernels (gemm_f64.cuh).  v0 is a split-K GEMM over the
+// Cholesky index with partial sums added in a fixed order, so results do not
+// depend on the device.  The matrix exponential is scaling and squaring of
+// a truncated Taylor series (Moler and Van Loan, "Nineteen dubious ways to
+// compute the exponential of a matrix, twenty-five years later", SIAM Review
+// 45 (2003), method 3), with the degree chosen from the remainder bound
+// theta^(m+1) / (m+1)! * e^theta <= 2^-53 for theta = ||A / 2^s||_1 <= 1/2.
+// The eigensolver is the cyclic two-sided Jacobi method in the parallel
+// round-robin ordering (Golub and Van Loan, Matrix Computations, 4th ed.,
+// sections 8.5.2 and 8.5.5), run by one CTA on a copy of the matrix.
+#include <cuda_runtime.h>
+
+#include <math.h>
+
+#include "afqmc_b200.h"
+#include "common.cuh"
+#include "gemm_f64.cuh"
+#include "profile.cuh"
+
+namespace afq {
+namespace {
+
+constexpr int kUnsegS = 1 << 30;
+using CfgS = F64Cfg<2, 4, 4, 2>;    // 64 x 64, 8 warps: rot_chol, rot_h1, expm
+using CfgV0 = F64Cfg<4, 8, 4, 2>;   // 128 x 128, 8 warps: v0
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+inline bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+inline long long even(long long x) { return (x + 1) & ~1LL; }
+
+// C[z] = alpha * sum_{b in batches of z} A[b] B[b] (+ beta Cin[z]) (+ diag on the diagonal)
+struct DgemmArgs {
+  F64Operand A, B;
+  int M, N, K;
+  int nbatch;      // input batches
+  int bsum;        // 0: output z uses input batch z; > 0: output z sums batches [z bsum, (z+1) bsum)
+  double alpha, beta, diag;
+  const double* cin;
+  long long ldcin, cin_bs;
+  double* C;
+  long long ldc, c_bs;
+};
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT) dgemm_kernel(DgemmArgs a) {
+  extern __shared__ double smem[];
+  const int m0 = blockIdx.x * Cfg::BM, n0 = blockIdx.y * Cfg::BN, z = blockIdx.z;
+  double acc[Cfg::FM][Cfg::FN][2];
+  f64_zero<Cfg>(acc);
+  int b0 = z, b1 = z + 1;
+  if (a.bsum > 0) {
+    b0 = z * a.bsum;
+    b1 = min(a.nbatch, b0 + a.bsum);
+  }
+  for (int b = b0; b < b1; ++b)
+    f64_mainloop<Cfg, B_KMAJOR>(acc, a.A, a.B, a.M, a.N, 0, a.K, m0, n0, b, false, smem);
+  double* Cz = a.C + (long long)z * a.c_bs;
+  const double* Iz = a.cin ? a.cin + (long long)z * a.cin_bs : nullptr;
+  f64_foreach<Cfg>(acc, m0, n0, [&](int m, int n, double v0, double v1) {
+    if (m >= a.M) return;
+    double v[2] = {v0, v1};
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int c = n + j;
+      if (c >= a.N) continue;
+      double x = a.alpha * v[j];
+      if (Iz) x += a.beta * Iz[(long long)m * a.ldcin + c];
+      if (m == c) x += a.diag;
+      Cz[(long long)m * a.ldc + c] = x;
+    }
+  });
+}
+
+template <class Cfg>
+cudaError_t dgemm(const DgemmArgs& a, int zdim, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(dgemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)Cfg::SMEM);
+  if (e != cudaSuccess) return e;
+  dim3 grid((a.M + Cfg::BM - 1) / Cfg::BM, (a.N + Cfg::BN - 1) / Cfg::BN, zdim);
+  ProfScope ps(K_MISC, st);
+  dgemm_kernel<Cfg><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+// plain square product C = alpha A B (+ diag I), n x n row-major, ld n
+cudaError_t square_gemm(int n, const double* A, const double* B, double alpha, double diag, double* C,
+                        cudaStream_t st) {
+  DgemmArgs a{};
+  a.A = F64Operand{A, n, 0, 0, kUnsegS};
+  a.B = F64Operand{B, n, 0, 0, kUnsegS};
+  a.M = a.N = a.K = n;
+  a.nbatch = 1;
+  a.alpha = alpha;
+  a.diag = diag;
+  a.C = C;
+  a.ldc = n;
+  return dgemm<CfgS>(a, 1, st);
+}
+
+// ---------------------------------------------------------------------------
+// measurement intermediates
+// ---------------------------------------------------------------------------
+// h1[s] <- (h1[s] + h1[s]^T)/2 in place for both spins; hrot[0] = RHF: (h1[0]+h1[1])/2,
+// UHF: h1[0]; hrot[1] = h1[1] (UHF only); mot[s] = mo[s]^T (no x N)
+__global__ void sym_kernel(int n, double* h1, double* hrot, int uhf) {
+  const long long nn = (long long)n * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / n), j = (int)(e % n);
+    if (i > j) continue;
+    double a[2];
+    for (int s = 0; s < 2; ++s) {
+      a[s] = 0.5 * (h1[s * nn + (long long)i * n + j] + h1[s * nn + (long long)j * n + i]);
+    }
+    for (int s = 0; s < 2; ++s) {
+      h1[s * nn + (long long)i * n + j] = a[s];
+      h1[s * nn + (long long)j * n + i] = a[s];
+    }
+    if (uhf) {
+      for (int s = 0; s < 2; ++s) {
+        hrot[s * nn + (long long)i * n + j] = a[s];
+        hrot[s * nn + (long long)j * n + i] = a[s];
+      }
+    } else {
+      const double v = 0.5 * (a[0] + a[1]);
+      hrot[(long long)i * n + j] = v;
+      hrot[(long long)j * n + i] = v;
+    }
+  }
+}
+
+__global__ void transpose_kernel(int rows, int cols, const double* in, double* out) {
+  const long long nn = (long long)rows * cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e / cols), c = (int)(e % cols);
+    out[(long long)c * rows + r] = in[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// propagation intermediates
+// ---------------------------------------------------------------------------
+// s_g = sum_ij L_g[ij] rho[ij] (one CTA per g); mf[g] = (0, s_g)
+__global__ void __launch_bounds__(256) mf_kernel(long long nn, const double* chol, const double* rho,
+                                                 double* mf) {
+  __shared__ double red[8];
+  const int g = blockIdx.x;
+  const double* L = chol + (long long)g * nn;
+  double s = 0.0;
+  for (long long e = threadIdx.x; e < nn; e += blockDim.x) s += L[e] * rho[e];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) {
+    mf[2 * g] = 0.0;
+    mf[2 * g + 1] = s;
+  }
+}
+
+// h0_prop = -h0 - sum_g mf_g^2 / 2 with mf_g = i s_g: -h0 + sum s_g^2 / 2 (real), one CTA
+__global__ void __launch_bounds__(256) h0prop_kernel(int G, const double* mf, double h0,
+                                                     double* h0p) {
+  __shared__ double red[8];
+  double s = 0.0;
+  for (int g = threadIdx.x; g < G; g += blockDim.x) s += mf[2 * g + 1] * mf[2 * g + 1];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) {
+    h0p[0] = -h0 + 0.5 * s;
+    h0p[1] = 0.0;
+  }
+}
+
+// v1 partial sums: part[z][ij] = sum_{g in z-th range} (-s_g) L_g[ij]
+__global__ void __launch_bounds__(256) v1_kernel(long long nn, int G, int gper, const double* chol,
+                                                 const double* mf, double* part) {
+  const int z = blockIdx.y;
+  const int g0 = z * gper, g1 = min(G, g0 + gper);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    for (int g = g0; g < g1; ++g) v -= mf[2 * g + 1] * chol[(long long)g * nn + e];
+    part[(long long)z * nn + e] = v;
+  }
+}
+
+// out[s] = scale * (h[s] - 1/2 sum_z v0part[z] - sum_z v1part[z]) for s < np
+// (h: restricted (h1[0]+h1[1])/2, unrestricted h1[s])
+__global__ void hmod_kernel(long long nn, int np, const double* h1, int avg, const double* v0p,
+                            int nz0, const double* v1p, int nz1, double scale, double* out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    double v0 = 0.0, v1 = 0.0;
+    for (int z = 0; z < nz0; ++z) v0 += v0p[(long long)z * nn + e];
+    for (int z = 0; z < nz1; ++z) v1 += v1p[(long long)z * nn + e];
+    const double v = 0.5 * v0 + v1;
+    for (int s = 0; s < np; ++s) {
+      const double h = avg ? 0.5 * (h1[e] + h1[nn + e]) : h1[s * nn + e];
+      out[s * nn + e] = scale * (h - v);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// matrix exponential helpers
+// ---------------------------------------------------------------------------
+// ||A||_1 (largest column sum of |a_ij|), one CTA
+__global__ void __launch_bounds__(256) norm1_kernel(int n, const double* A, double* out) {
+  __shared__ double red[256];
+  double m = 0.0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += fabs(A[(long long)i * n + j]);
+    m = fmax(m, s);
+  }
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+// P = I + B / m  (the innermost Horner factor)
+__global__ void horner_init_kernel(int n, const double* B, double inv_m, double* P) {
+  const long long nn = (long long)n * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / n), j = (int)(e % n);
+    P[e] = B[e] * inv_m + (i == j ? 1.0 : 0.0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi eigensolver (one CTA)
+// ---------------------------------------------------------------------------
+constexpr int kJacobiThreads = 1024;
+constexpr int kJacobiMaxSweeps = 40;
+constexpr int kJacobiMaxN = 2048;
+
+// round-robin pairing: position k of round r (n even, positions 0..n-1)
+__device__ __forceinline__ int rr_index(int k, int r, int n) {
+  if (k == 0) return 0;
+  return 1 + (k - 1 + r) % (n - 1);
+}
+
+// A (n x n, ld n, symmetric) is overwritten; V (n x n) receives the
+// eigenvectors as columns; evals/evecs: sorted descending.  n_pad = n rounded
+// up to even; the padding index (n) is a phantom with no rotations.
+__global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(int n, double* A, double* V,
+                                                                double* evals, double* evecs,
+                                                                int* sweeps_out) {
+  extern __shared__ double js[];
+  const int np = (n + 1) & ~1;
+  const int npair = np / 2;
+  double* cs = js;                 // [npair] c
+  double* sn = cs + npair;         // [npair] s
+  int* pp = reinterpret_cast<int*>(sn + npair);  // [npair] p
+  int* qq = pp + npair;                           // [npair] q
+  __shared__ double red[32];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const long long nn = (long long)n * n;
+  for (long long e = tid; e < nn; e += nt) V[e] = ((e / n) == (e % n)) ? 1.0 : 0.0;
+  double fro = 0.0;
+  for (long long e = tid; e < nn; e += nt) fro += A[e] * A[e];
+  fro = block_sum(fro, red);
+  const double tol2 = fro * 1e-30;
+  int sweep = 0;
+  for (; sweep < kJacobiMaxSweeps; ++sweep) {
+    double off = 0.0;
+    for (long long e = tid; e < nn; e += nt)
+      if ((e / n) != (e % n)) off += A[e] * A[e];
+    off = block_sum(off, red);
+    if (off <= tol2 || fro == 0.0) break;
+    for (int r = 0; r < np - 1; ++r) {
+      // rotation parameters of this round (GVL Algorithm 8.5.1, sym.schur2)
+      for (int k = tid; k < npair; k += nt) {
+        int p = rr_index(k, r, np), q = rr_index(np - 1 - k, r, np);
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
+        }
+        double c = 1.0, s = 0.0;
+        if (q < n) {
+          const double apq = A[(long long)p * n + q];
+          const double app = A[(long long)p * n + p], aqq = A[(long long)q * n + q];
+          if (apq != 0.0 && fabs(apq) > 1e-300) {
+            const double tau = (aqq - app) / (2.0 * apq);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = 1.0 / sqrt(1.0 + t * t);
+            s = t * c;
+          }
+        }
+        cs[k] = c;
+        sn[k] = s;
+        pp[k] = p;
+        qq[k] = q < n ? q : -1;
+      }
+      __syncthreads();
+      // columns: A <- A J, V <- V J
+      for (long long it = tid; it < (long long)npair * n; it += nt) {
+        const int k = (int)(it / n), i = (int)(it % n);
+        const int p = pp[k], q = qq[k];
+        if (q < 0 || sn[k] == 0.0) continue;
+        const double c = cs[k], s = sn[k];
+        double* ar = A + (long long)i * n;
+        const double x = ar[p], y = ar[q];
+        ar[p] = c * x - s * y;
+        ar[q] = s * x + c * y;
+        double* vr = V + (long long)i * n;
+        const double u = vr[p], w = vr[q];
+        vr[p] = c * u - s * w;
+        vr[q] = s * u + c * w;
+      }
+      __syncthreads();
+      // rows: A <- J^T A
+      for (long long it = tid; it < (long long)npair * n; it += nt) {
+        const int k = (int)(it / n), j = (int)(it % n);
+        const int p = pp[k], q = qq[k];
+        if (q < 0 || sn[k] == 0.0) continue;
+        const double c = cs[k], s = sn[k];
+        const double x = A[(long long)p * n + j], y = A[(long long)q * n + j];
+        A[(long long)p * n + j] = c * x - s * y;
+        A[(long long)q * n + j] = s * x + c * y;
+      }
+      __syncthreads();
+      // the rotated pair's off-diagonal element is zero by construction
+      for (int k = tid; k < npair; k += nt) {
+        const int p = pp[k], q = qq[k];
+        if (q < 0 || sn[k] == 0.0) continue;
+        A[(long long)p * n + q] = 0.0;
+        A[(long long)q * n + p] = 0.0;
+      }
+      __syncthreads();
+    }
+  }
+  // descending order: rank of eigenvalue i (ties by index)
+  for (int i = tid; i < n; i += nt) {
+    const double li = A[(long long)i * n + i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double lj = A[(long long)j * n + j];
+      if (lj > li || (lj == li && j < i)) ++rank;
+    }
+    evals[rank] = li;
+    for (int row = 0; row < n; ++row) evecs[(long long)row * n + rank] = V[(long long)row * n + i];
+  }
+  if (tid == 0 && sweeps_out) *sweeps_out = sweep;
+}
+
+int vsplits(int n, int G, int* bsum) {
+  const int tiles = ((n + CfgV0::BM - 1) / CfgV0::BM) * ((n + CfgV0::BN - 1) / CfgV0::BN);
+  int want = (296 + tiles - 1) / tiles;
+  if (want > G) want = G;
+  if (want < 1) want = 1;
+  const int per = (G + want - 1) / want;
+  *bsum = per;
+  return (G + per - 1) / per;
+}
+
+constexpr int kV1Split = 16;
+
+}  // namespace
+}  // namespace afq
+
+using namespace afq;
+
+extern "C" {
+
+int afq_intermediates_workspace_size(int32_t norb, int32_t nchol, size_t* bytes) {
+  if (!bytes) return AFQ_ERR_NULL;
+  if (norb <= 0 || nchol <= 0 || norb > kJacobiMaxN) return AFQ_ERR_SHAPE;
+  const long long nn = (long long)norb * norb;
+  int bsum = 0;
+  const int nz = vsplits(norb, nchol, &bsum);
+  // v0 partials, v1 partials, hmod (2 spins), three expm buffers, the norm, eigensolver copy + V
+  long long d = nz * nn + (long long)kV1Split * nn + 2 * nn + 3 * nn + 2 + 2 * nn + 8;
+  d += 64;  // alignment slack between sub-buffers
+  *bytes = (size_t)d * sizeof(double);
+  return AFQ_OK;
+}
+
+int afq_measurement_intermediates(int32_t norb, const int32_t nocc[2], int32_t nchol, int32_t trial_type,
+                                  const double* const mo[2], double* h1, const double* chol,
+                                  double* const rot_h1[2], double* const rot_chol[2], void* work,
+                                  size_t work_bytes, void* stream) {
+  if (!nocc || !mo || !h1 || !chol || !rot_h1 || !rot_chol || !work) return AFQ_ERR_NULL;
+  if (trial_type != AFQ_TRIAL_RHF && trial_type != AFQ_TRIAL_UHF) return AFQ_ERR_ARG;
+  const int ns = trial_type == AFQ_TRIAL_UHF ? 2 : 1;
+  if (norb <= 0 || nchol <= 0) return AFQ_ERR_SHAPE;
+  for (int s = 0; s < ns; ++s) {
+    if (nocc[s] <= 0 || nocc[s] > norb) return AFQ_ERR_SHAPE;
+    if (!mo[s] || !rot_h1[s] || !rot_chol[s]) return AFQ_ERR_NULL;
+  }
+  size_t need = 0;
+  afq_intermediates_workspace_size(norb, nchol, &need);
+  if (work_bytes < need) return AFQ_ERR_WORKSPACE;
+  if (!al16(work)) return AFQ_ERR_ALIGN;
+  cudaStream_t st = as_stream(stream);
+  const int n = norb;
+  const long long nn = (long long)n * n;
+  double* hrot = static_cast<double*>(work);  // 2 nn
+  double* mot = hrot + even(2 * nn);          // no x n per spin (<= nn each)
+  {
+    ProfScope ps(K_MISC, st);
+    sym_kernel<<<(int)((nn + 255) / 256), 256, 0, st>>>(n, h1, hrot, ns == 2);
+    if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+  }
+  for (int s = 0; s < ns; ++s) {
+    const int no = nocc[s];
+    double* mt = mot + s * even(nn);
+    {
+      ProfScope ps(K_MISC, st);
+      transpose_kernel<<<(int)(((long long)n * no + 255) / 256), 256, 0, st>>>(n, no, mo[s], mt);
+      if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+    }
+    // rot_h1[s] = mo^T h (no x n)
+    DgemmArgs a{};
+    a.A = F64Operand{mt, n, 0, 0, kUnsegS};
+    a.B = F64Operand{hrot + s * nn, n, 0, 0, kUnsegS};
+    a.M = no;
+    a.N = n;
+    a.K = n;
+    a.nbatch = 1;
+    a.alpha = 1.0;
+    a.C = rot_h1[s];
+    a.ldc = n;
+    if (dgemm<CfgS>(a, 1, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    // rot_chol[s][g] = mo^T L_g (no x n), batched over g
+    DgemmArgs b{};
+    b.A = F64Operand{mt, n, 0, 0, kUnsegS};
+    b.B = F64Operand{chol, n, nn, 0, kUnsegS};
+    b.M = no;
+    b.N = n;
+    b.K = n;
+    b.nbatch = nchol;
+    b.alpha = 1.0;
+    b.C = rot_chol[s];
+    b.ldc = n;
+    b.c_bs = (long long)no * n;
+    if (dgemm<CfgS>(b, nchol, st) != cudaSuccess) return AFQ_ERR_CUDA;
+  }
+  return AFQ_OK;
+}
+
+int afq_expm(int32_t n, const double* A, double scale, double* out, void* work, size_t work_bytes,
+             void* stream) {
+  if (!A || !out || !work) return AFQ_ERR_NULL;
+  if (n <= 0 || n > kJacobiMaxN) return AFQ_ERR_SHAPE;
+  const long long nn = (long long)n * n;
+  if (work_bytes < (size_t)(2 * even(nn) + 2) * sizeof(double)) return AFQ_ERR_WORKSPACE;
+  if (!al16(work)) return AFQ_ERR_ALIGN;
+  if (out == A) return AFQ_ERR_ARG;
+  cudaStream_t st = as_stream(stream);
+  double* P = static_cast<double*>(work);
+  double* Q = P + even(nn);
+  double* nrm = Q + even(nn);
+  const int blocks = (int)((nn + 255) / 256);
+  {
+    ProfScope ps(K_MISC, st);
+    norm1_kernel<<<1, 256, 0, st>>>(n, A, nrm);
+    if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+  }
+  double theta0 = 0.0;
+  if (cudaMemcpyAsync(&theta0, nrm, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return AFQ_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return AFQ_ERR_CUDA;
+  theta0 *= fabs(scale);
+  if (!isfinite(theta0)) return AFQ_ERR_ARG;
+  int s = 0;
+  while (theta0 / ldexp(1.0, s) > 0.5 && s < 1000) ++s;
+  const double theta = theta0 / ldexp(1.0, s);
+  // smallest degree m with theta^(m+1)/(m+1)! e^theta <= 2^-53
+  int m = 1;
+  {
+    double term = theta * theta / 2.0;  // theta^(m+1)/(m+1)! for m = 1
+    while (m < 30 && term * exp(theta) > ldexp(1.0, -53)) {
+      ++m;
+      term *= theta / (m + 1);
+    }
+  }
+  const double bscale = scale / ldexp(1.0, s);
+  // Horner: P = I + B/m ; P <- I + B P / k for k = m-1 .. 1 ; B = bscale A
+  {
+    ProfScope ps(K_MISC, st);
+    horner_init_kernel<<<blocks, 256, 0, st>>>(n, A, bscale / m, P);
+    if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+  }
+  double* cur = P;
+  double* nxt = Q;
+  for (int k = m - 1; k >= 1; --k) {
+    if (square_gemm(n, A, cur, bscale / k, 1.0, nxt, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    double* t = cur;
+    cur = nxt;
+    nxt = t;
+  }
+  // squaring
+  for (int i = 0; i < s; ++i) {
+    double* dst = (i == s - 1) ? out : nxt;
+    if (square_gemm(n, cur, cur, 1.0, 0.0, dst, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    if (i == s - 1) cur = out;
+    else {
+      double* t = cur;
+      cur = nxt;
+      nxt = t;
+    }
+  }
+  if (s == 0 && cudaMemcpyAsync(out, cur, nn * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return AFQ_ERR_CUDA;
+  return AFQ_OK;
+}
+
+int afq_propagation_intermediates(int32_t norb, int32_t nchol, int32_t walker_type, const double* h1,
+                                  const double* rdm1, const double* chol, double h0, double dt,
+                                  double* mf_shifts, double* h0_prop, double* exp_h1, void* work,
+                                  size_t work_bytes, void* stream) {
+  if (!h1 || !rdm1 || !chol || !mf_shifts || !h0_prop || !exp_h1 || !work) return AFQ_ERR_NULL;
+  if (walker_type != AFQ_RESTRICTED && walker_type != AFQ_UNRESTRICTED) return AFQ_ERR_ARG;
+  if (norb <= 0 || nchol <= 0 || norb > kJacobiMaxN) return AFQ_ERR_SHAPE;
+  size_t need = 0;
+  afq_intermediates_workspace_size(norb, nchol, &need);
+  if (work_bytes < need) return AFQ_ERR_WORKSPACE;
+  if (!al16(work) || !al16(rdm1) || !al16(chol)) return AFQ_ERR_ALIGN;
+  cudaStream_t st = as_stream(stream);
+  const int n = norb, G = nchol;
+  const long long nn = (long long)n * n;
+  const int np = walker_type == AFQ_UNRESTRICTED ? 2 : 1;
+  int bsum = 0;
+  const int nz = vsplits(n, G, &bsum);
+  double* v0p = static_cast<double*>(work);
+  double* v1p = v0p + even(nz * nn);
+  double* hm = v1p + even((long long)kV1Split * nn);
+  double* ew = hm + even(2 * nn);  // expm workspace: 3 nn + 2
+  const int blocks = (int)((nn + 255) / 256);
+  {
+    ProfScope ps(K_MISC, st);
+    // rdm1 is (2, n, n): rho = rdm1[0] + rdm1[1], formed in the expm scratch
+    hmod_kernel<<<blocks, 256, 0, st>>>(nn, 1, rdm1, 1, nullptr, 0, nullptr, 0, 2.0, ew);
+    mf_kernel<<<G, 256, 0, st>>>(nn, chol, ew, mf_shifts);
+    h0prop_kernel<<<1, 256, 0, st>>>(G, mf_shifts, h0, h0_prop);
+    const int gper = (G + kV1Split - 1) / kV1Split;
+    v1_kernel<<<dim3((unsigned)((nn + 255) / 256), kV1Split), 256, 0, st>>>(nn, G, gper, chol,
+                                                                             mf_shifts, v1p);
+    if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+  }
+  // v0 partials: part[z] = sum_{g in z} L_g L_g
+  {
+    DgemmArgs a{};
+    a.A = F64Operand{chol, n, nn, 0, kUnsegS};
+    a.B = F64Operand{chol, n, nn, 0, kUnsegS};
+    a.M = a.N = a.K = n;
+    a.nbatch = G;
+    a.bsum = bsum;
+    a.alpha = 1.0;
+    a.C = v0p;
+    a.ldc = n;
+    a.c_bs = nn;
+    if (dgemm<CfgV0>(a, nz, st) != cudaSuccess) return AFQ_ERR_CUDA;
+  }
+  // h1_mod per spin, then exp(-dt/2 h1_mod)
+  {
+    ProfScope ps(K_MISC, st);
+    hmod_kernel<<<blocks, 256, 0, st>>>(nn, np, h1, np == 1, v0p, nz, v1p, kV1Split, 1.0, hm);
+    if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+  }
+  for (int s = 0; s < np; ++s) {
+    const int rc = afq_expm(n, hm + s * nn, -0.5 * dt, exp_h1 + s * nn, ew,
+                            (size_t)(3 * even(nn) + 2) * sizeof(double), stream);
+    if (rc != AFQ_OK) return rc;
+  }
+  return AFQ_OK;
+}
+
+int afq_eigh_desc(int32_t n, const double* A, double* evals, double* evecs, void* work,
+                  size_t work_bytes, void* stream) {
+  if (!A || !evals || !evecs || !work) return AFQ_ERR_NULL;
+  if (n <= 0 || n > kJacobiMaxN) return AFQ_ERR_SHAPE;
+  const long long nn = (long long)n * n;
+  if (work_bytes < (size_t)(2 * even(nn) + 8) * sizeof(double)) return AFQ_ERR_WORKSPACE;
+  if (!al16(work)) return AFQ_ERR_ALIGN;
+  cudaStream_t st = as_stream(stream);
+  double* Ac = static_cast<double*>(work);
+  double* V = Ac + even(nn);
+  int* sweeps = reinterpret_cast<int*>(V + even(nn));
+  if (cudaMemcpyAsync(Ac, A, nn * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return AFQ_ERR_CUDA;
+  const int npair = ((n + 1) & ~1) / 2;
+  const size_t smem = (size_t)npair * (2 * sizeof(double) + 2 * sizeof(int));
+  if (cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return AFQ_ERR_CUDA;
+  ProfScope ps(K_MISC, st);
+  jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(n, Ac, V, evals, evecs, sweeps);
+  return cudaGetLastError() == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
+}
+
+}  // extern "C"

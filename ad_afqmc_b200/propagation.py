@@ -235,40 +235,28 @@ class propagator_afqmc(propagator):
         return prop_data
 
     def _build_propagation_intermediates(self, ham_data: dict, trial, wave_data: dict) -> dict:
-        """mf_shifts, h0_prop, *_fp, exp_h1 (propagation.py:378-438), on the device."""
-        n = trial.norb
-        rdm1 = to_dev(wave_data["rdm1"])
-        rdm1 = rdm1[0] + rdm1[1]
+        """mf_shifts, h0_prop, *_fp, exp_h1 (propagation.py:378-438), by
+        afq_propagation_intermediates (v0 and the exponentials on the FP64
+        tensor cores)."""
+        from . import intermediates
+
         ham_data["chol"] = to_dev(ham_data["chol"])
-        L = ham_data["chol"].reshape(-1, n, n)
-        G = L.shape[0]
-        mf = 1j * (ham_data["chol"] @ rdm1.reshape(-1)).to(torch.complex128)
+        ham_data["h1"] = to_dev(ham_data["h1"])
+        unrestricted = self.walker_type == "unrestricted"
+        mf, h0_prop, exp_h1 = intermediates.propagation(trial.norb, ham_data["h1"], wave_data["rdm1"],
+                                                        ham_data["chol"], float(ham_data["h0"]), self.dt,
+                                                        unrestricted)
         ham_data["mf_shifts"] = mf
-        h0 = float(ham_data["h0"])
-        h0_prop = -h0 - torch.sum(mf**2) / 2.0
         ham_data["h0_prop"] = h0_prop
         na, nb = trial.nelec
         ene0 = float(ham_data.get("ene0", 0.0))
-        if self.walker_type == "unrestricted":
+        if unrestricted:
             ham_data["mf_shifts_fp"] = torch.stack((mf / na / 2.0, mf / nb / 2.0))
             ham_data["h0_prop_fp"] = torch.stack(((h0_prop + ene0) / na / 2.0, (h0_prop + ene0) / nb / 2.0))
         else:
             ham_data["mf_shifts_fp"] = mf / 2.0 / na
             ham_data["h0_prop_fp"] = (h0_prop + ene0) / na / 2.0
-        # v0 = 1/2 sum_g L_g L_g  as one GEMM over (g, k)
-        v0 = 0.5 * (L.permute(1, 0, 2).reshape(n, G * n) @ L.reshape(G * n, n))
-        mf_r = (1j * mf).real
-        v1 = (mf_r @ ham_data["chol"]).reshape(n, n)
-        h1 = to_dev(ham_data["h1"])
-        if self.walker_type == "unrestricted":
-            h1_mod = h1 - torch.stack([v0 + v1, v0 + v1])
-            ham_data["exp_h1"] = torch.stack([
-                torch.linalg.matrix_exp(-self.dt * h1_mod[0] / 2.0),
-                torch.linalg.matrix_exp(-self.dt * h1_mod[1] / 2.0),
-            ]).contiguous()
-        else:
-            h1_mod = (h1[0] + h1[1]) / 2.0 - v0 - v1
-            ham_data["exp_h1"] = torch.linalg.matrix_exp(-self.dt * h1_mod / 2.0).contiguous()
+        ham_data["exp_h1"] = exp_h1
         drop_engines(ham_data)
         return ham_data
 

@@ -4,8 +4,9 @@ Method names, arguments and the ``ham_data`` / ``wave_data`` keys follow the
 reference classes ``rhf`` (wavefunctions.py:1038-1235) and ``uhf``
 (:1238-1499); the batched dispatch on the walker type follows the base class
 ``wave_function`` (:19-493).  Overlap, Green's function, force bias and local
-energy run in libafqmc_b200 (FP64); the half-rotated intermediates are built
-on the device with torch GEMMs once per solve.
+energy run in libafqmc_b200 (FP64), and so do the half-rotated
+intermediates and the natural orbitals of the initial walkers
+(``intermediates.py``).
 """
 
 from __future__ import annotations
@@ -16,7 +17,7 @@ from typing import List, Optional, Sequence, Tuple
 
 import torch
 
-from . import _lib
+from . import _lib, intermediates
 from ._engine import drop_engines, get_engine, small_work, to_dev
 from .walkers import RHFWalkers, UHFWalkers, walker_batch
 
@@ -143,11 +144,11 @@ class wave_function:
         rdm1 = self.get_rdm1(wave_data)
         na, nb = self.nelec
         if walker_type == "restricted":
-            nat = torch.linalg.eigh(rdm1[0] + rdm1[1])[1].flip(-1)[:, :na]
+            nat = intermediates.natural_orbitals(rdm1[0] + rdm1[1], na)
             return RHFWalkers(nat.to(torch.complex128).unsqueeze(0).repeat(n_walkers, 1, 1))
         if walker_type == "unrestricted":
-            up = torch.linalg.eigh(rdm1[0])[1].flip(-1)[:, :na].to(torch.complex128)
-            dn = torch.linalg.eigh(rdm1[1])[1].flip(-1)[:, :nb].to(torch.complex128)
+            up = intermediates.natural_orbitals(rdm1[0], na).to(torch.complex128)
+            dn = intermediates.natural_orbitals(rdm1[1], nb).to(torch.complex128)
             return UHFWalkers([up.unsqueeze(0).repeat(n_walkers, 1, 1),
                                dn.unsqueeze(0).repeat(n_walkers, 1, 1)])
         raise Exception("Unknown walker_type.")
@@ -158,13 +159,6 @@ class wave_function:
     def __hash__(self) -> int:
         """wavefunctions.py:492-493."""
         return hash(tuple(self.__dict__.values()))
-
-
-def _sym(h1: torch.Tensor) -> torch.Tensor:
-    h = h1.clone()
-    h[0] = (h1[0] + h1[0].T) / 2.0
-    h[1] = (h1[1] + h1[1].T) / 2.0
-    return h
 
 
 @dataclass
@@ -190,14 +184,15 @@ class rhf(wave_function):
         return torch.stack([mo @ mo.T, mo @ mo.T])
 
     def _build_measurement_intermediates(self, ham_data: dict, wave_data: dict) -> dict:
-        """rot_h1 = C^H (h1a + h1b)/2, rot_chol[g] = C^H L_g (wavefunctions.py:1215-1232)."""
-        h1 = _sym(to_dev(ham_data["h1"]))
-        ham_data["h1"] = h1
-        mo = to_dev(wave_data["mo_coeff"])
-        ham_data["rot_h1"] = (mo.T @ ((h1[0] + h1[1]) / 2.0)).contiguous()
+        """h1 symmetrized, rot_h1 = C^H (h1a + h1b)/2, rot_chol[g] = C^H L_g
+        (wavefunctions.py:1215-1232), by afq_measurement_intermediates."""
         ham_data["chol"] = to_dev(ham_data["chol"])
-        L = ham_data["chol"].reshape(-1, self.norb, self.norb)
-        ham_data["rot_chol"] = torch.matmul(mo.T, L).contiguous()
+        mo = to_dev(wave_data["mo_coeff"])
+        h1, rh1, rc = intermediates.measurement(self.norb, self.nelec, ham_data["h1"], ham_data["chol"],
+                                                [mo], uhf=False)
+        ham_data["h1"] = h1
+        ham_data["rot_h1"] = rh1[0]
+        ham_data["rot_chol"] = rc[0]
         wave_data.pop("_afq_mo", None)
         drop_engines(ham_data)
         return ham_data
@@ -251,14 +246,15 @@ class uhf(wave_function):
         return torch.stack([m0 @ m0.T, m1 @ m1.T])
 
     def _build_measurement_intermediates(self, ham_data: dict, wave_data: dict) -> dict:
-        """rot_h1[s] = C_s^H h1[s], rot_chol[s][g] = C_s^H L_g (wavefunctions.py:1472-1496)."""
-        h1 = _sym(to_dev(ham_data["h1"]))
-        ham_data["h1"] = h1
-        m0, m1 = to_dev(wave_data["mo_coeff"][0]), to_dev(wave_data["mo_coeff"][1])
-        ham_data["rot_h1"] = [(m0.T @ h1[0]).contiguous(), (m1.T @ h1[1]).contiguous()]
+        """h1 symmetrized, rot_h1[s] = C_s^H h1[s], rot_chol[s][g] = C_s^H L_g
+        (wavefunctions.py:1472-1496), by afq_measurement_intermediates."""
         ham_data["chol"] = to_dev(ham_data["chol"])
-        L = ham_data["chol"].reshape(-1, self.norb, self.norb)
-        ham_data["rot_chol"] = [torch.matmul(m0.T, L).contiguous(), torch.matmul(m1.T, L).contiguous()]
+        mos = [to_dev(wave_data["mo_coeff"][0]), to_dev(wave_data["mo_coeff"][1])]
+        h1, rh1, rc = intermediates.measurement(self.norb, self.nelec, ham_data["h1"], ham_data["chol"],
+                                                mos, uhf=True)
+        ham_data["h1"] = h1
+        ham_data["rot_h1"] = rh1
+        ham_data["rot_chol"] = rc
         wave_data.pop("_afq_mo", None)
         drop_engines(ham_data)
         return ham_data

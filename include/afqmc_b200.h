@@ -298,6 +298,59 @@ typedef struct afq_tuning {
 int afq_set_tuning(const afq_dims* d, const afq_tuning* t);
 int afq_get_tuning(const afq_dims* d, afq_tuning* out);
 
+/* ---- Per-solve Hamiltonian intermediates (FP64, device pointers) ----------
+ * These replace the set-up half of the walker path, run once per solve:
+ * every contraction runs on the FP64 tensor cores of this library.  They
+ * take their own scratch `work` of afq_intermediates_workspace_size() bytes
+ * (16-byte aligned); nothing is allocated.  Layouts are the reference's:
+ * h1 (2, N, N), chol (G, N*N), mo (N, nocc[s]), rdm1 (2, N, N), all row-major. */
+int afq_intermediates_workspace_size(int32_t norb, int32_t nchol, size_t* bytes);
+
+/* h1[s] <- (h1[s] + h1[s]^T) / 2 in place for both spins; rot_h1[s] (nocc[s], N)
+ * = mo[s]^T h with h = (h1[0] + h1[1]) / 2 for an RHF trial (one sector) and
+ * h = h1[s] for a UHF trial (two); rot_chol[s] (G, nocc[s], N) with
+ * rot_chol[s][g] = mo[s]^T L_g.  Replaces rhf._build_measurement_intermediates
+ * (wavefunctions.py:1215-1232) and uhf._build_measurement_intermediates
+ * (:1472-1496). */
+int afq_measurement_intermediates(int32_t norb, const int32_t nocc[2], int32_t nchol,
+                                  int32_t trial_type, const double* const mo[2], double* h1,
+                                  const double* chol, double* const rot_h1[2],
+                                  double* const rot_chol[2], void* work, size_t work_bytes,
+                                  void* stream);
+
+/* rho = rdm1[0] + rdm1[1]; mf_shifts (G,) complex128 = i sum(L_g o rho);
+ * h0_prop (one complex128) = -h0 - sum(mf_shifts^2) / 2; v0 = 1/2 sum_g L_g L_g;
+ * v1 = sum_g Re(i mf_g) L_g; exp_h1 = expm(-dt/2 h1_mod) with h1_mod =
+ * (h1[0] + h1[1]) / 2 - v0 - v1 for restricted walkers (exp_h1: (N, N)) or
+ * h1[s] - v0 - v1 per spin for unrestricted walkers (exp_h1: (2, N, N)).
+ * h1 is the symmetrized one (afq_measurement_intermediates).  Synchronizes
+ * `stream` once per exponential (the scaling exponent is chosen on the host).
+ * Replaces propagator_afqmc._build_propagation_intermediates
+ * (propagation.py:378-438); mf_shifts_fp and h0_prop_fp are scalar multiples
+ * of these and left to the caller. */
+int afq_propagation_intermediates(int32_t norb, int32_t nchol, int32_t walker_type, const double* h1,
+                                  const double* rdm1, const double* chol, double h0, double dt,
+                                  double* mf_shifts, double* h0_prop, double* exp_h1, void* work,
+                                  size_t work_bytes, void* stream);
+
+/* out (n, n) = expm(scale * A) for a real (n, n) matrix A (out must not alias
+ * A): scaling and squaring of a truncated Taylor series whose degree follows
+ * from the remainder bound for ||scale A / 2^s||_1 <= 1/2.  Synchronizes
+ * `stream` once.  Replaces jax.scipy.linalg.expm in propagation.py:422-438.
+ * work: at least 2 n^2 + 2 doubles (afq_intermediates_workspace_size covers it). */
+int afq_expm(int32_t n, const double* A, double scale, double* out, void* work, size_t work_bytes,
+             void* stream);
+
+/* Eigenpairs of a real symmetric (n, n) matrix A, eigenvalues in descending
+ * order into evals (n,) and the eigenvectors as the columns of evecs (n, n),
+ * in the same order (cyclic Jacobi, n <= 2048).  The natural orbitals of
+ * wave_function.get_init_walkers (wavefunctions.py:427-466) are the first
+ * nocc columns for rdm1[0] + rdm1[1] (restricted walkers) or rdm1[s]
+ * (unrestricted).  Within a degenerate eigenspace the basis may differ from
+ * LAPACK's (as it may between LAPACK builds).  work: 2 n^2 + 8 doubles. */
+int afq_eigh_desc(int32_t n, const double* A, double* evals, double* evecs, void* work,
+                  size_t work_bytes, void* stream);
+
 /* Device-side failure status of a workspace (no counterpart in the reference,
  * whose XLA kernels have no waits of their own; its only guards are the
  * numerical masks of propagation.py:321-331 and the driver's check of the
