@@ -348,6 +348,28 @@ def summarize(results: List[Result], wall: float) -> Dict:
             "mean_blocks": float(np.mean([r.n_blocks for r in results]))}
 
 
+def setup_latency(precision: str = "mixed", norb: int = 250, nchol: int = 1250, n_walkers: int = 256,
+                  reps: int = 3) -> Dict:
+    """Per-request set-up time of the largest served fragment (N = 250, G =
+    1250): integrals from the client's pinned buffer to the device,
+    measurement and propagation intermediates, initial walkers and energy,
+    and the capture of the block graph, on one stream (median of ``reps``)."""
+    no = int(round(norb / 4))
+    sys_ = make_system(norb, (no, no), nchol, 4242, "rhf", chol_scale=fragment_chol_scale(norb)).pin()
+    times = []
+    for k in range(reps + 1):
+        req = Request(k, sys_, n_walkers, 100 + k)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sv = Solve(req, precision, 10, 0.0)
+        sv.stream.synchronize()
+        if k > 0:  # the first one also loads kernels
+            times.append(time.perf_counter() - t0)
+        del sv
+    return {"norb": norb, "nchol": nchol, "nocc": no, "n_walkers": n_walkers,
+            "setup_ms_median": 1e3 * float(np.median(times)), "setup_ms": [1e3 * t for t in times]}
+
+
 def bench(rate: float = 20.0, duration: float = 10.0, precision: str = "mixed", slots: int = 16,
           max_blocks: int = 40, stop_rule: str = "sem", lno: bool = False, baseline: bool = True) -> Dict:
     """The serving workload: Poisson arrivals at ``rate``/s for ``duration``

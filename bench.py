@@ -664,6 +664,7 @@ def main():
 
             fragments["serving"] = serving.bench(rate=20.0, duration=args.serving_duration,
                                                  precision=args.precision)
+            fragments["setup"] = serving.setup_latency(args.precision)
         except Exception as exc:
             fragments["serving"] = {"error": f"{type(exc).__name__}: {exc}"}
         torch.cuda.empty_cache()
