@@ -117,6 +117,7 @@ class Solve:
         self.stream = stream if stream is not None else torch.cuda.Stream()
         self.lno = req.prjlo is not None
         self.host = torch.empty(3, dtype=torch.float64).pin_memory()
+        self.host_status = torch.zeros(1, dtype=torch.int32).pin_memory()
         self.event = torch.cuda.Event()
         sys_ = req.system
         with torch.cuda.stream(self.stream):
@@ -145,6 +146,7 @@ class Solve:
                 self.block.replay()
             out = self.block.replay()
             self.host[: out.numel()].copy_(out, non_blocking=True)
+            self.host_status.copy_(self.block.status, non_blocking=True)
             self.event.record(self.stream)
         self.in_flight = True
 
@@ -153,6 +155,8 @@ class Solve:
         if not self.in_flight or not self.event.query():
             return False
         self.in_flight = False
+        if int(self.host_status[0]) != 0:
+            raise _lib.AfqError(f"request {self.req.rid}: a device-side wait timed out; its blocks are invalid")
         self.energies.append(float(self.host[0]))
         self.weights.append(float(self.host[1]))
         if self.lno:
