@@ -135,6 +135,11 @@ _SIGS = {
                                 C.c_void_p], C.c_int),
     "afq_set_tuning": ([C.POINTER(afq_dims), C.c_void_p], C.c_int),
     "afq_get_tuning": ([C.POINTER(afq_dims), C.POINTER(afq_tuning)], C.c_int),
+    "afq_batch_table_size": ([C.c_int32, C.c_void_p, C.POINTER(C.c_size_t)], C.c_int),
+    "afq_batch_create": ([C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                          C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
+    "afq_batch_propagate_constrained": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p], C.c_int),
+    "afq_batch_destroy": ([C.c_void_p], C.c_int),
     "afq_intermediates_workspace_size": ([C.c_int32, C.c_int32, C.POINTER(C.c_size_t)], C.c_int),
     "afq_measurement_intermediates": ([C.c_int32, C.c_int32 * 2, C.c_int32, C.c_int32, C.c_void_p * 2,
                                        C.c_void_p, C.c_void_p, C.c_void_p * 2, C.c_void_p * 2, C.c_void_p,

@@ -20,7 +20,7 @@ from typing import Dict, List, Optional
 import torch
 
 from . import hamiltonian, propagation, wavefunctions
-from .graphs import BatchGraph, BlockGraph
+from .graphs import BatchGraph, BlockGraph, GroupedBatchGraph
 from .synthetic import make_fragment_batch, make_system
 
 
@@ -96,6 +96,17 @@ def bench(n_fragments: int = 64, precision: str = "mixed", n_prop_steps: int = 1
     fb.capture()
     ms_batch = _time(fb.step, reps)
     extra: Dict = {}
+    if precision != "fp64":
+        # all fragments in one graph with the steps in grouped launches (persistent grouped
+        # tcgen05 GEMMs over (fragment, tile) work lists), from the same state onward
+        gb = GroupedBatchGraph(fb.blocks, n_streams=n_streams).capture(warmup=1)
+        ms_grouped = _time(gb.replay, reps)
+        gb.check_status()
+        extra.update({"grouped_graph_ms": ms_grouped,
+                      "walker_steps_per_s_grouped": ws / (ms_grouped / 1e3),
+                      "launches_per_block_grouped": gb.launches_per_block,
+                      "speedup_grouped_vs_forked_streams": ms_batch / ms_grouped})
+        del gb
     if tune:
         from .autotune import Autotuner, tune_batch
 

@@ -38,42 +38,6 @@ int check_walkers(const Layout& L, const double* const w[2]) {
   return AFQ_OK;
 }
 
-GreenArgs green_args_mo(const Layout& L, const double* const mo[2], double* work,
-                        const double* const walkers[2]) {
-  GreenArgs a{};
-  a.N = L.N;
-  a.W = L.W;
-  a.ns = L.ns;
-  a.wscal = work + L.w_wscal;
-  a.gpl = nullptr;
-  a.ldg = L.Kfb;
-  for (int s = 0; s < L.ns; ++s) {
-    a.sec[s].walk = walkers[s];
-    a.sec[s].mo = mo[L.uhf_trial ? s : 0];
-    a.sec[s].rh1 = nullptr;
-    a.sec[s].no = L.no[s];
-    a.sec[s].koff = L.koff[s];
-    a.sec[s].theta = nullptr;
-    a.sec[s].gout = nullptr;
-    for (int i = 0; i < 3; ++i) a.sec[s].gtb[i] = nullptr;
-    a.sec[s].ldtb = L.Nb;
-  }
-  a.npc = L.npc;
-  for (int i = 0; i < 3; ++i) a.gplb[i] = nullptr;
-  a.ldgb = L.Kb;
-  a.sbuf = nullptr;
-  a.sstride = (long long)L.nomax * L.nomax;
-  return a;
-}
-
-GreenArgs green_args(const Layout& L, const double* prep, double* work,
-                     const double* const walkers[2]) {
-  const double* mo[2] = {prep + L.p_mo[0], prep + L.p_mo[1]};
-  GreenArgs a = green_args_mo(L, mo, work, walkers);
-  a.sbuf = work + L.w_s;  // the full workspace: S goes through the warp-level inverse
-  return a;
-}
-
 int check_small(const afq_dims* d, Layout& L, void* work, size_t work_bytes) {
   int rc = make_layout(d, L);
   if (rc != AFQ_OK) return rc;

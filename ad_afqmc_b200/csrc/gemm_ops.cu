@@ -59,15 +59,14 @@ __global__ void __launch_bounds__(Cfg::NT) fb_gemm_kernel(F64Operand A, F64Opera
 // ---------------------------------------------------------------------------
 // field preparation (one CTA per walker)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) prep_kernel(int W, int G, long long Gpad, int splitk,
-                                                   const double* fbpart, double alpha,
-                                                   const double* fields, const double* mf,
-                                                   double sdt, double* xt, double* wscal,
-                                                   double* fb_out, int npc, bf16* xb0, bf16* xb1,
-                                                   bf16* xb2, long long ldxb) {
+__device__ __forceinline__ void prep_body(int W, int G, long long Gpad, int splitk,
+                                          const double* fbpart, double alpha, const double* fields,
+                                          const double* mf, double sdt, double* xt, double* wscal,
+                                          double* fb_out, int npc, bf16* xb0, bf16* xb1, bf16* xb2,
+                                          long long ldxb, int w) {
   bf16* const xb[3] = {xb0, xb1, xb2};
   __shared__ double red[4 * 8];
-  const int w = blockIdx.x, tid = threadIdx.x;
+  const int tid = threadIdx.x;
   const long long zs = 2LL * W * Gpad;
   double sr = 0, si = 0, br = 0, bi = 0;
   for (int g = tid; g < G; g += blockDim.x) {
@@ -116,6 +115,23 @@ __global__ void __launch_bounds__(256) prep_kernel(int W, int G, long long Gpad,
       s[3] = bi;
     }
   }
+}
+
+__global__ void __launch_bounds__(256) prep_kernel(int W, int G, long long Gpad, int splitk,
+                                                   const double* fbpart, double alpha,
+                                                   const double* fields, const double* mf,
+                                                   double sdt, double* xt, double* wscal,
+                                                   double* fb_out, int npc, bf16* xb0, bf16* xb1,
+                                                   bf16* xb2, long long ldxb) {
+  prep_body(W, G, Gpad, splitk, fbpart, alpha, fields, mf, sdt, xt, wscal, fb_out, npc, xb0, xb1,
+            xb2, ldxb, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256) prep_kernel_grouped(const PrepArgs* A, BlockMap m, int step) {
+  int local;
+  const PrepArgs& a = A[block_owner(m, blockIdx.x, local)];
+  prep_body(a.W, a.G, a.Gpad, a.splitk, a.fbpart, a.alpha, a.fields + (long long)step * a.field_step,
+            a.mf, a.sdt, a.xt, a.wscal, nullptr, a.npc, a.xb[0], a.xb[1], a.xb[2], a.ldxb, local);
 }
 
 // ---------------------------------------------------------------------------
@@ -455,6 +471,12 @@ cudaError_t launch_fb_gemm(const Layout& L, const double* prep, double* work, cu
   fb_gemm_kernel<Cfg><<<grid, Cfg::NT, Cfg::SMEM, st>>>(A, B, M, N, (int)K, kchunk,
                                                         work + L.w_fbpart, L.Gpad,
                                                         2LL * L.W * L.Gpad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prep_grouped(const PrepArgs* args, const BlockMap& m, int step, cudaStream_t st) {
+  ProfScope ps(K_PREP, st);
+  prep_kernel_grouped<<<m.start[m.n], 256, 0, st>>>(args, m, step);
   return cudaGetLastError();
 }
 

@@ -127,9 +127,8 @@ __device__ double2 gauss_jordan_cta(double2* S, double2* colk, int* perm, double
 
 // mode 0: the whole computation; 1: S = C^T W only, into a.sbuf; 2: Theta
 // and its outputs from S^-1 in a.sbuf (the inverse and det by gj_kernel)
-__global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int mode) {
+__device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, int sct) {
   extern __shared__ double2 sm[];
-  const int w = blockIdx.x, sct = blockIdx.y;
   const GreenSector& S_ = a.sec[sct];
   const int N = a.N, no = S_.no, tid = threadIdx.x;
   constexpr int T = kGreenThreads;
@@ -393,10 +392,9 @@ __device__ __forceinline__ int gj_pivot(double2 v0, double2 v1, bool ok0, bool o
 //    which every thread reads in step k+1; warps 1..7 update all other
 //    elements.  det = product of the pivots times the permutation's sign.
 // At most 64 rows (no <= 64, checked by the caller).
-__global__ void __launch_bounds__(kGreenThreads, 4)
-    gj_kernel(int W, int no0, int no1, double* sbuf, long long sstride, int bstride, double* wscal) {
+__device__ __forceinline__ void gj_body(int W, int no0, int no1, double* sbuf, long long sstride,
+                                        int bstride, double* wscal, int w, int sct) {
   extern __shared__ double2 gsm[];
-  const int w = blockIdx.x, sct = blockIdx.y;
   const int no = sct ? no1 : no0;
   const int ld = no | 1;
   const int nn = no * no;
@@ -529,9 +527,30 @@ __global__ void __launch_bounds__(kGreenThreads, 4)
   }
 }
 
-__global__ void ovlp_combine_kernel(int W, int ns, int mult, const double* wscal, double* out,
-                                    int out_stride) {
-  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int mode) {
+  green_body(a, mode, blockIdx.x, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(kGreenThreads) green_kernel_grouped(const GreenArgs* A, BlockMap m,
+                                                                      int mode) {
+  int local;
+  const GreenArgs& a = A[block_owner(m, blockIdx.x, local)];
+  green_body(a, mode, local % a.W, local / a.W);
+}
+
+__global__ void __launch_bounds__(kGreenThreads, 4)
+    gj_kernel(int W, int no0, int no1, double* sbuf, long long sstride, int bstride, double* wscal) {
+  gj_body(W, no0, no1, sbuf, sstride, bstride, wscal, blockIdx.x, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(kGreenThreads, 4) gj_kernel_grouped(const GjArgs* A, BlockMap m) {
+  int local;
+  const GjArgs& a = A[block_owner(m, blockIdx.x, local)];
+  gj_body(a.W, a.no0, a.no1, a.sbuf, a.sstride, a.bstride, a.wscal, local % a.W, local / a.W);
+}
+
+__device__ __forceinline__ void ovlp_body(int W, int ns, int mult, const double* wscal, double* out,
+                                          int out_stride, int w) {
   if (w >= W) return;
   const double2 d0 = make_double2(wscal[(long long)w * 16 + 4], wscal[(long long)w * 16 + 5]);
   double2 o;
@@ -545,16 +564,57 @@ __global__ void ovlp_combine_kernel(int W, int ns, int mult, const double* wscal
   out[(long long)w * out_stride + 1] = o.y;
 }
 
+__global__ void ovlp_combine_kernel(int W, int ns, int mult, const double* wscal, double* out,
+                                    int out_stride) {
+  ovlp_body(W, ns, mult, wscal, out, out_stride, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__global__ void ovlp_combine_grouped(const OvlpArgs* A, BlockMap m) {
+  int local;
+  const OvlpArgs& a = A[block_owner(m, blockIdx.x, local)];
+  ovlp_body(a.W, a.ns, a.mult, a.wscal, a.out, a.out_stride, local * blockDim.x + threadIdx.x);
+}
+
 }  // namespace
+
+size_t green_smem_bytes(int nomax) {
+  const int sdmax = 2 * nomax + ((20 - (2 * nomax) % 16) % 16);  // padded walker-row stride (doubles)
+  return (size_t(nomax) * nomax + 64) * sizeof(double2) + 2 * size_t(kRowChunk) * sdmax * sizeof(double) +
+         2 * size_t(kRowChunk) * nomax * sizeof(double) + size_t(kRowChunk) * (nomax + 1) * sizeof(double2);
+}
+
+// two row-padded copies of S (row stride nomax | 1) and two scaled pivot rows
+size_t gj_smem_bytes(int nomax) { return (2 * size_t(nomax) * (nomax | 1) + 128) * sizeof(double2); }
+
+cudaError_t launch_green_grouped(const GreenArgs* args, const BlockMap& m, int mode, size_t smem,
+                                 cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(green_kernel_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  ProfScope ps(K_GREEN, st);
+  green_kernel_grouped<<<m.start[m.n], kGreenThreads, smem, st>>>(args, m, mode);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gj_grouped(const GjArgs* args, const BlockMap& m, size_t smem, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(gj_kernel_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  ProfScope ps(K_GREEN, st);
+  gj_kernel_grouped<<<m.start[m.n], kGreenThreads, smem, st>>>(args, m);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ovlp_grouped(const OvlpArgs* args, const BlockMap& m, cudaStream_t st) {
+  ProfScope ps(K_MISC, st);
+  ovlp_combine_grouped<<<m.start[m.n], 256, 0, st>>>(args, m);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   int nomax = 0;
   for (int s = 0; s < a.ns; ++s) nomax = a.sec[s].no > nomax ? a.sec[s].no : nomax;
-  const int sdmax = 2 * nomax + ((20 - (2 * nomax) % 16) % 16);  // padded walker-row stride (doubles)
-  const size_t smem = (size_t(nomax) * nomax + 64) * sizeof(double2) +
-                      2 * size_t(kRowChunk) * sdmax * sizeof(double) +
-                      2 * size_t(kRowChunk) * nomax * sizeof(double) +
-                      size_t(kRowChunk) * (nomax + 1) * sizeof(double2);
+  const size_t smem = green_smem_bytes(nomax);
   cudaError_t e = cudaFuncSetAttribute(green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
@@ -570,9 +630,8 @@ cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   // S into a.sbuf; warp-level inverse and det; Theta and its outputs
   green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 1);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  // two row-padded copies of S (row stride nomax | 1) and two scaled pivot rows
   const int bstride = nomax * (nomax | 1);
-  const size_t gsmem = (2 * size_t(bstride) + 128) * sizeof(double2);
+  const size_t gsmem = gj_smem_bytes(nomax);
   if ((e = cudaFuncSetAttribute(gj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem)) !=
       cudaSuccess)
     return e;

@@ -20,6 +20,9 @@
 //                (wavefunctions.py:1128-1174, 1331-1363)
 #include <cuda.h>
 
+#include <cstring>
+#include <vector>
+
 #include "afqmc_b200.h"
 #include "common.cuh"
 #include "ops.h"
@@ -84,12 +87,13 @@ __global__ void transpose_split_kernel(const double* src, long long R, long long
 }
 
 // walker (W, N, nc) doubles -> pieces of its transpose (W, nc rows, K = N) with row stride ld
-__global__ void walker_t_kernel(const double* wk, int N, int nc, int np, bf16* p0, bf16* p1,
-                                bf16* p2, long long ld, long long bstride, float* acc) {
+__device__ __forceinline__ void walker_t_body(const double* wk, int N, int nc, int np, bf16* p0,
+                                              bf16* p1, bf16* p2, long long ld, long long bstride,
+                                              float* acc, int bx, int by, int bz) {
   __shared__ double tile[32][33];
   bf16* P[3] = {p0, p1, p2};
-  const int b = blockIdx.z;
-  const int p0_ = blockIdx.x * 32, n0 = blockIdx.y * 32;
+  const int b = bz;
+  const int p0_ = bx * 32, n0 = by * 32;
   const double* src = wk + (long long)b * N * nc;
   for (int i = threadIdx.y; i < 32; i += blockDim.y) {
     const int p = p0_ + i, n = n0 + threadIdx.x;
@@ -104,6 +108,20 @@ __global__ void walker_t_kernel(const double* wk, int N, int nc, int np, bf16* p
       acc[((long long)b * nc + n) * N + p] = (float)x;  // identity term of the first half-step
     }
   }
+}
+
+__global__ void walker_t_kernel(const double* wk, int N, int nc, int np, bf16* p0, bf16* p1,
+                                bf16* p2, long long ld, long long bstride, float* acc) {
+  walker_t_body(wk, N, nc, np, p0, p1, p2, ld, bstride, acc, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+__global__ void walker_t_grouped(const WalkerTArgs* A, BlockMap m) {
+  int local;
+  const WalkerTArgs& a = A[block_owner(m, blockIdx.x, local)];
+  const int per = a.gx * a.gy;
+  const int bz = local / per, r = local - bz * per;
+  walker_t_body(a.wk, a.N, a.nc, a.np, a.p[0], a.p[1], a.p[2], a.ld, a.bstride, a.acc, r % a.gx,
+                r / a.gx, bz);
 }
 
 // ---------------------------------------------------------------------------
@@ -418,6 +436,15 @@ void base_shape(UmmaParams<Epi>& P, int npc, int M, int N, int K, int batch, int
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// While a batch is built, the GEMMs of one solve are recorded here (final
+// parameters, tile width, epilogue warpgroups) instead of launched.
+struct SinkRec {
+  int prof, bn, eg;
+  UmmaShape shape;
+  std::vector<unsigned char> bytes;  // the UmmaParams<Epi> block
+};
+thread_local std::vector<SinkRec>* g_sink = nullptr;
+
 // `extra`: epilogue scratch bytes per epilogue warpgroup
 template <int BN, int EG = 1, class Epi>
 int run(UmmaParams<Epi>& P, size_t extra, cudaStream_t st, int prof_id, const afq_tuning& T) {
@@ -431,6 +458,17 @@ int run(UmmaParams<Epi>& P, size_t extra, cudaStream_t st, int prof_id, const af
   }
   if (P.s.stages < 2) return AFQ_ERR_SHAPE;
   if (T.max_stages >= 2 && P.s.stages > T.max_stages) P.s.stages = T.max_stages;
+  if (g_sink) {
+    SinkRec r;
+    r.prof = prof_id;
+    r.bn = BN;
+    r.eg = EG;
+    r.shape = P.s;
+    r.bytes.resize(sizeof(P));
+    std::memcpy(r.bytes.data(), &P, sizeof(P));
+    g_sink->push_back(std::move(r));
+    return AFQ_OK;
+  }
   int ctas = sm_count();
   if (T.grid_cap > 0 && T.grid_cap < ctas) ctas = T.grid_cap;
   ProfScope ps(prof_id, st);
@@ -571,7 +609,7 @@ int fb_launch(const Layout& L, const double* prep, double* work, cudaStream_t st
   for (int z = ks; z < L.splitk; ++z)
     if (cudaMemsetAsync(work + L.w_fbpart + z * 2LL * L.W * L.Gpad, 0,
                         sizeof(double) * 2LL * L.W * L.Gpad, st) != cudaSuccess)
-      return AFQ_ERR_CUDA;
+      return AFQ_ERR_CUDA;  // (while recording a batch: once, on the legacy stream, at build time)
   P.epi.part = work + L.w_fbpart;
   P.epi.ld = L.Gpad;
   P.epi.zstride = 2LL * L.W * L.Gpad;
@@ -622,7 +660,7 @@ static int propagate_one(const Layout& L, const double* prep, double* work, doub
   piece_ptrs(work, L.v_bt[0], L.v_bt_ps, L.npc, b0);
   piece_ptrs(work, L.v_bt[1], L.v_bt_ps, L.npc, b1);
   const long long btbs = 2LL * L.nomax * L.Kv;
-  {
+  if (!g_sink) {  // a batch launches the operand preparation of all its solves together
     ProfScope ps(K_MISC, st);
     dim3 grid((N + 31) / 32, (nc + 31) / 32, L.W);
     walker_t_kernel<<<grid, dim3(32, 8), 0, st>>>(wk, N, nc, L.npc, b0[0], b0[1], b0[2], L.Kv,
@@ -690,5 +728,208 @@ int mixed_exchange(const Layout& L, const double* prep, double* work, int s, cud
     default: return exch_launch<32>(L, prep, work, s, st);
   }
 }
+
+cudaError_t launch_walker_t_grouped(const WalkerTArgs* args, const BlockMap& m, cudaStream_t st) {
+  ProfScope ps(K_MISC, st);
+  walker_t_grouped<<<m.start[m.n], dim3(32, 8), 0, st>>>(args, m);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// batches: the step's GEMMs of many solves, one persistent launch per group
+// ---------------------------------------------------------------------------
+namespace {
+
+// one grouped launch: entries of the same kind, tile width, epilogue
+// warpgroups, ring depth and operand/epilogue layout
+struct GroupLaunch {
+  int prof, bn, eg;
+  UmmaShape shape0;
+  const void* entries;  // device
+  int n, stages;
+  int start[kUmmaMaxGroup + 1];
+};
+
+template <int BN, int EG, class Epi>
+int launch_group_as(const GroupLaunch& g, cudaStream_t st) {
+  UmmaGroup<Epi> G;
+  G.entries = static_cast<const UmmaParams<Epi>*>(g.entries);
+  G.n = g.n;
+  G.stages = g.stages;
+  for (int i = 0; i <= g.n; ++i) G.start[i] = g.start[i];
+  ProfScope ps(g.prof, st);
+  return launch_umma_group<BN, EG>(G, g.shape0, sm_count(), st) == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
+}
+
+template <class Epi, int EG>
+int launch_group_bn(const GroupLaunch& g, cudaStream_t st) {
+  switch (g.bn) {
+    case 16: return launch_group_as<16, EG, Epi>(g, st);
+    case 32: return launch_group_as<32, EG, Epi>(g, st);
+    case 48: return launch_group_as<48, EG, Epi>(g, st);
+    case 64: return launch_group_as<64, EG, Epi>(g, st);
+    case 80: return launch_group_as<80, EG, Epi>(g, st);
+    case 96: return launch_group_as<96, EG, Epi>(g, st);
+    case 128: return launch_group_as<128, EG, Epi>(g, st);
+    default: return AFQ_ERR_SHAPE;
+  }
+}
+
+int launch_group(const GroupLaunch& g, cudaStream_t st) {
+  if (g.prof == K_FB) {
+    if (g.eg != 1 || (g.bn != 64 && g.bn != 128)) return AFQ_ERR_SHAPE;
+    return g.bn == 64 ? launch_group_as<64, 1, FbEpiU>(g, st) : launch_group_as<128, 1, FbEpiU>(g, st);
+  }
+  if (g.prof == K_VHS) {
+    if (g.eg != 1 || (g.bn != 64 && g.bn != 128)) return AFQ_ERR_SHAPE;
+    return g.bn == 64 ? launch_group_as<64, 1, VhsEpiU>(g, st) : launch_group_as<128, 1, VhsEpiU>(g, st);
+  }
+  if (g.prof == K_PROP) {
+    if (g.eg == 1) return launch_group_bn<PropEpiU, 1>(g, st);
+    if (g.eg == 2) return launch_group_bn<PropEpiU, 2>(g, st);
+    if (g.eg == 3) return launch_group_bn<PropEpiU, 3>(g, st);
+  }
+  return AFQ_ERR_SHAPE;
+}
+
+constexpr int kMaxPropLaunches = 34;  // n_exp_terms (<= 32) + 1, per spin sector
+
+size_t rec_bytes_max() {
+  size_t b = sizeof(UmmaParams<FbEpiU>);
+  if (sizeof(UmmaParams<VhsEpiU>) > b) b = sizeof(UmmaParams<VhsEpiU>);
+  if (sizeof(UmmaParams<PropEpiU>) > b) b = sizeof(UmmaParams<PropEpiU>);
+  return (b + 255) & ~size_t(255);
+}
+
+}  // namespace
+
+struct UmmaBatch {
+  std::vector<GroupLaunch> fb, vhs;
+  std::vector<GroupLaunch> prop[2][kMaxPropLaunches];
+  int nprop = 0;
+};
+
+size_t umma_batch_table_bytes(int n, const Layout* L, int n_exp_terms) {
+  size_t cnt = 0;
+  for (int f = 0; f < n; ++f) cnt += 2 + (size_t)L[f].np * (n_exp_terms + 1);
+  return cnt * rec_bytes_max() + 4096;
+}
+
+int umma_batch_create(int n, const Layout* L, const double* const* prep, double* const* work,
+                      double* const* walkers0, double* const* walkers1, int n_exp_terms,
+                      void* table, size_t table_bytes, UmmaBatch** out) {
+  if (n < 1 || n > kMaxBatch || n_exp_terms + 1 > kMaxPropLaunches) return AFQ_ERR_SHAPE;
+  // record every solve's GEMMs with the solo code path
+  std::vector<std::vector<SinkRec>> recs(n);
+  for (int f = 0; f < n; ++f) {
+    std::vector<SinkRec> sink;
+    g_sink = &sink;
+    double* wk[2] = {walkers0[f], walkers1[f]};
+    int rc = mixed_fb_gemm(L[f], prep[f], work[f], 0);
+    if (rc == AFQ_OK) rc = mixed_vhs_gemm(L[f], prep[f], work[f], 0);
+    if (rc == AFQ_OK) rc = mixed_propagate_walkers(L[f], prep[f], work[f], wk, n_exp_terms, 0);
+    g_sink = nullptr;
+    if (rc != AFQ_OK) return rc;
+    recs[f] = std::move(sink);
+  }
+  if (cudaStreamSynchronize(0) != cudaSuccess) return AFQ_ERR_CUDA;  // the split-K zero fills
+  // slot of record r of solve f: 0 fb, 1 vhs, 2 + s*(n_exp_terms+1) + i propagator i of sector s
+  const int nprop = n_exp_terms <= 1 ? 2 : n_exp_terms + 1;
+  for (int f = 0; f < n; ++f)
+    if ((int)recs[f].size() != 2 + L[f].np * nprop) return AFQ_ERR_SHAPE;
+  std::vector<unsigned char> host(table_bytes, 0);
+  size_t off = 0;
+  UmmaBatch* b = new UmmaBatch();
+  b->nprop = nprop;
+  // group the records of one slot across solves
+  auto group_slot = [&](int slot_kind, int sector, int index, std::vector<GroupLaunch>& dst) -> int {
+    std::vector<std::pair<const SinkRec*, int>> items;  // (record, solve)
+    for (int f = 0; f < n; ++f) {
+      int r;
+      if (slot_kind == 0) r = 0;
+      else if (slot_kind == 1) r = 1;
+      else {
+        if (sector >= L[f].np) continue;
+        r = 2 + sector * nprop + index;
+      }
+      items.push_back({&recs[f][r], f});
+    }
+    std::vector<bool> done(items.size(), false);
+    for (size_t i = 0; i < items.size(); ++i) {
+      if (done[i]) continue;
+      const SinkRec& k = *items[i].first;
+      GroupLaunch g{};
+      g.prof = k.prof;
+      g.bn = k.bn;
+      g.eg = k.eg;
+      g.shape0 = k.shape;
+      g.stages = k.shape.stages;
+      g.n = 0;
+      g.start[0] = 0;
+      off = (off + 255) & ~size_t(255);
+      const size_t first = off;
+      for (size_t j = i; j < items.size(); ++j) {
+        if (done[j]) continue;
+        const SinkRec& r = *items[j].first;
+        if (r.prof != k.prof || r.bn != k.bn || r.eg != k.eg || r.shape.stages != k.shape.stages ||
+            r.shape.npa != k.shape.npa || r.shape.npb != k.shape.npb ||
+            r.shape.ngroups != k.shape.ngroups || r.shape.epi_bytes != k.shape.epi_bytes ||
+            r.bytes.size() != k.bytes.size())
+          continue;
+        if (off + r.bytes.size() > table_bytes) return AFQ_ERR_WORKSPACE;
+        std::memcpy(host.data() + off, r.bytes.data(), r.bytes.size());
+        off += r.bytes.size();
+        const UmmaShape& S = r.shape;
+        g.start[g.n + 1] = g.start[g.n] + S.batch * S.ksplit * S.mt * S.nt;
+        ++g.n;
+        done[j] = true;
+      }
+      g.entries = static_cast<unsigned char*>(table) + first;
+      dst.push_back(g);
+    }
+    return AFQ_OK;
+  };
+  int rc = group_slot(0, 0, 0, b->fb);
+  if (rc == AFQ_OK) rc = group_slot(1, 0, 0, b->vhs);
+  for (int sct = 0; sct < 2 && rc == AFQ_OK; ++sct)
+    for (int i = 0; i < nprop && rc == AFQ_OK; ++i) rc = group_slot(2, sct, i, b->prop[sct][i]);
+  if (rc == AFQ_OK && cudaMemcpy(table, host.data(), off, cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = AFQ_ERR_CUDA;
+  if (rc != AFQ_OK) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return AFQ_OK;
+}
+
+int umma_batch_fb(const UmmaBatch* b, cudaStream_t st) {
+  for (const GroupLaunch& g : b->fb) {
+    const int rc = launch_group(g, st);
+    if (rc != AFQ_OK) return rc;
+  }
+  return AFQ_OK;
+}
+
+int umma_batch_vhs(const UmmaBatch* b, cudaStream_t st) {
+  for (const GroupLaunch& g : b->vhs) {
+    const int rc = launch_group(g, st);
+    if (rc != AFQ_OK) return rc;
+  }
+  return AFQ_OK;
+}
+
+int umma_batch_prop(const UmmaBatch* b, int sector, int index, cudaStream_t st) {
+  if (sector < 0 || sector > 1 || index < 0 || index >= b->nprop) return AFQ_ERR_ARG;
+  for (const GroupLaunch& g : b->prop[sector][index]) {
+    const int rc = launch_group(g, st);
+    if (rc != AFQ_OK) return rc;
+  }
+  return AFQ_OK;
+}
+
+int umma_batch_nprop(const UmmaBatch* b) { return b->nprop; }
+
+void umma_batch_destroy(UmmaBatch* b) { delete b; }
 
 }  // namespace afq

@@ -100,19 +100,67 @@ inline int umma_pick_stages(int bn, int npa, int npb, size_t extra) {
   return 0;
 }
 
-template <int BN, class Epi, int EG>
-__global__ void __launch_bounds__(64 + 128 * EG, 1)
-    umma_gemm_kernel(const __grid_constant__ UmmaParams<Epi> P) {
+// Several independent GEMMs of one kind (one per fragment of a batch) in one
+// persistent launch: entry e owns global tiles [start[e], start[e+1]).  The
+// entries share BN, the number of bf16 pieces, the accumulator groups, the
+// epilogue scratch and the ring depth; everything else (tensor maps, sizes,
+// epilogue pointers, error flag) is per entry.  The entries live in device
+// memory (their tensor maps are read by TMA from global memory).
+constexpr int kUmmaMaxGroup = 64;
+
+template <class Epi>
+struct UmmaGroup {
+  const UmmaParams<Epi>* entries;
+  int n;
+  int stages;
+  int start[kUmmaMaxGroup + 1];
+};
+
+// Tile sources of the kernel body: one GEMM from the kernel parameter, or a
+// group of GEMMs from device memory (entry found by binary search).
+template <class Epi>
+struct UmmaOne {
+  const UmmaParams<Epi>& P;
+  __device__ int stages() const { return P.s.stages; }
+  __device__ int tiles() const { return P.s.batch * P.s.ksplit * P.s.mt * P.s.nt; }
+  __device__ const UmmaParams<Epi>& first() const { return P; }
+  __device__ const UmmaParams<Epi>& entry(int it, int& local) const {
+    local = it;
+    return P;
+  }
+};
+
+template <class Epi>
+struct UmmaMany {
+  const UmmaGroup<Epi>& G;
+  __device__ int stages() const { return G.stages; }
+  __device__ int tiles() const { return G.start[G.n]; }
+  __device__ const UmmaParams<Epi>& first() const { return G.entries[0]; }
+  __device__ const UmmaParams<Epi>& entry(int it, int& local) const {
+    int lo = 0, hi = G.n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (G.start[mid] <= it) lo = mid;
+      else hi = mid - 1;
+    }
+    local = it - G.start[lo];
+    return G.entries[lo];
+  }
+};
+
+template <int BN, class Epi, int EG, class Src>
+__device__ __forceinline__ void umma_body(const Src& src) {
   static_assert(EG >= 1 && EG <= 3, "one to three epilogue warpgroups");
   constexpr int NBUF = EG > 2 ? EG : 2;  // accumulator buffers
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M=128");
   static_assert(umma_tmem_cols(BN) <= 512, "two accumulators must fit in TMEM");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const UmmaShape& S = P.s;
-  const int ST = S.stages;
+  const UmmaParams<Epi>& P0 = src.first();
+  const int ST = src.stages();
+  const int npa = P0.s.npa, npb = P0.s.npb, ngrp = P0.s.ngroups, epi_bytes = P0.s.epi_bytes;
   const uint32_t a_bytes = kUBM * 128, b_bytes = BN * 128;
-  const uint32_t stage_bytes = S.npa * a_bytes + S.npb * b_bytes;
+  const uint32_t stage_bytes = npa * a_bytes + npb * b_bytes;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + ST * stage_bytes);
   uint64_t* empty = full + ST;
   uint64_t* accf = empty + ST;
@@ -120,8 +168,8 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce + NBUF);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_slot + 1);
   uint8_t* epi_smem = reinterpret_cast<uint8_t*>(full) + 256;  // epilogue scratch
-  const uint32_t kCols = umma_tmem_cols(BN, P.s.ngroups, NBUF);
-  const uint32_t acc_stride = (uint32_t)(P.s.ngroups * BN);  // columns per accumulator buffer
+  const uint32_t kCols = umma_tmem_cols(BN, ngrp, NBUF);
+  const uint32_t acc_stride = (uint32_t)(ngrp * BN);  // columns per accumulator buffer
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -137,8 +185,8 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
     fence_barrier_init();
   }
   if (warp == 0 && lane == 0) {
-    for (int i = 0; i < S.npa; ++i) prefetch_tmap(&P.ta[i]);
-    for (int i = 0; i < S.npb; ++i) prefetch_tmap(&P.tb[i]);
+    for (int i = 0; i < npa; ++i) prefetch_tmap(&P0.ta[i]);
+    for (int i = 0; i < npb; ++i) prefetch_tmap(&P0.tb[i]);
   }
   if (warp == 1) tmem_alloc(tmem_slot, kCols);
   tc_fence_before();
@@ -146,10 +194,27 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
   tc_fence_after();
   const uint32_t tbase = *tmem_slot;
 
-  const int tiles = S.batch * S.ksplit * S.mt * S.nt;
-  auto fail = [&]() {
-    atomicExch(S.err, 1);
+  const int tiles = src.tiles();
+  auto fail = [&](int* err) {
+    atomicExch(err, 1);
     *abort_s = 1;
+  };
+  // (global iteration) -> entry, tile of the entry, and its coordinates
+  struct TileAt {
+    int z, mti, nti, b, k0, KB;
+  };
+  auto locate = [&](const UmmaShape& S, int local) {
+    const int etiles = S.batch * S.ksplit * S.mt * S.nt;
+    const int tile = S.reverse ? etiles - 1 - local : local;
+    TileAt t;
+    t.nti = tile % S.nt;
+    const int rest = tile / S.nt;
+    t.mti = rest % S.mt;
+    t.z = rest / S.mt;
+    t.b = t.z / S.ksplit;
+    t.k0 = (t.z % S.ksplit) * S.kchunk;
+    t.KB = (min(S.kchunk, S.K - t.k0) + kUBK - 1) / kUBK;
+    return t;
   };
 
   if (warp == 0) {
@@ -157,28 +222,29 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
       int stage = 0;
       uint32_t phase = 0;
       for (int it_ = blockIdx.x; it_ < tiles && !*abort_s; it_ += gridDim.x) {
-        const int tile = S.reverse ? tiles - 1 - it_ : it_;
-        const int nti = tile % S.nt, rest = tile / S.nt;
-        const int mti = rest % S.mt, z = rest / S.mt;
-        const int b = z / S.ksplit, k0 = (z % S.ksplit) * S.kchunk;
-        const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
-        for (int kb = 0; kb < KB; ++kb) {
-          if (!mbar_wait(&empty[stage], phase ^ 1)) { fail(); break; }
+        int local;
+        const UmmaParams<Epi>& P = src.entry(it_, local);
+        const UmmaShape& S = P.s;
+        const TileAt t = locate(S, local);
+        bool ok = true;
+        for (int kb = 0; kb < t.KB; ++kb) {
+          if (!mbar_wait(&empty[stage], phase ^ 1)) { fail(S.err); ok = false; break; }
           mbar_arrive_expect_tx(&full[stage], stage_bytes);
           uint8_t* sa = smem + stage * stage_bytes;
-          uint8_t* sb = sa + S.npa * a_bytes;
-          for (int i = 0; i < S.npa; ++i)
-            tma_load_3d(sa + i * a_bytes, &P.ta[i], &full[stage], k0 + kb * kUBK,
-                        mti * S.a_step, S.a_batched ? b : 0);
-          for (int j = 0; j < S.npb; ++j)
-            tma_load_3d(sb + j * b_bytes, &P.tb[j], &full[stage], k0 + kb * kUBK, nti * S.b_step,
-                        b);
+          uint8_t* sb = sa + npa * a_bytes;
+          for (int i = 0; i < npa; ++i)
+            tma_load_3d(sa + i * a_bytes, &P.ta[i], &full[stage], t.k0 + kb * kUBK,
+                        t.mti * S.a_step, S.a_batched ? t.b : 0);
+          for (int j = 0; j < npb; ++j)
+            tma_load_3d(sb + j * b_bytes, &P.tb[j], &full[stage], t.k0 + kb * kUBK,
+                        t.nti * S.b_step, t.b);
           if (++stage == ST) { stage = 0; phase ^= 1; }
         }
+        if (!ok) break;
       }
       // drain: wait (bounded) until the MMA side released every stage we filled
       for (int s = 0; s < ST; ++s) {
-        if (!mbar_wait(&empty[stage], phase ^ 1)) { fail(); break; }
+        if (!mbar_wait(&empty[stage], phase ^ 1)) { fail(P0.s.err); break; }
         if (++stage == ST) { stage = 0; phase ^= 1; }
       }
     }
@@ -190,29 +256,31 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
       int it = 0, t = 0;
       uint32_t uses[NBUF] = {};  // EG > 1: chunks accumulated so far in each buffer
       for (int it_ = blockIdx.x; it_ < tiles && !*abort_s; it_ += gridDim.x, ++t) {
-        const int tile = S.reverse ? tiles - 1 - it_ : it_;
-        const int k0 = ((tile / (S.nt * S.mt)) % S.ksplit) * S.kchunk;
-        const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
+        int local;
+        const UmmaParams<Epi>& P = src.entry(it_, local);
+        const UmmaShape& S = P.s;
+        const TileAt tl = locate(S, local);
+        const int KB = tl.KB;
         const int kc = S.kc > 0 ? S.kc : KB;
         bool ok = true;
         for (int c0 = 0; c0 < KB && ok; c0 += kc, ++it) {
           const int buf = EG > 1 ? (t % EG) : (it & 1);
           const uint32_t use = EG > 1 ? uses[buf]++ : (uint32_t)(it >> 1);
-          if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); ok = false; break; }
+          if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(S.err); ok = false; break; }
           tc_fence_after();
           const uint32_t dt = tbase + buf * acc_stride;
           const int c1 = min(KB, c0 + kc);
           for (int kb = c0; kb < c1; ++kb) {
-            if (!mbar_wait(&full[stage], phase)) { fail(); ok = false; break; }
+            if (!mbar_wait(&full[stage], phase)) { fail(S.err); ok = false; break; }
             tc_fence_after();
             const uint8_t* sa = smem + stage * stage_bytes;
-            const uint8_t* sb = sa + S.npa * a_bytes;
+            const uint8_t* sb = sa + npa * a_bytes;
             for (int p = 0; p < S.npairs; ++p) {
               const uint64_t ad = smem_desc_sw128(sa + S.pa[p] * a_bytes);
               const uint64_t bd = smem_desc_sw128(sb + S.pb[p] * b_bytes);
               // group 0: pair 0 alone; group 1 (if any): the remaining pairs
-              const int grp = (S.ngroups == 2 && p > 0) ? 1 : 0;
-              const int first = (p == 0) || (S.ngroups == 2 && p == 1);
+              const int grp = (ngrp == 2 && p > 0) ? 1 : 0;
+              const int first = (p == 0) || (ngrp == 2 && p == 1);
 #pragma unroll
               for (int ks = 0; ks < kUBK / 16; ++ks)
                 umma_bf16(dt + grp * BN, ad + 2 * ks, bd + 2 * ks, idesc,
@@ -231,29 +299,29 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
     const int sub = warp & 3;
     const int eg = (warp - 2) >> 2;  // epilogue warpgroup
     const int row = sub * 32 + lane;
-    uint8_t* escr = epi_smem + eg * S.epi_bytes;
+    uint8_t* escr = epi_smem + eg * epi_bytes;
     float* srow = reinterpret_cast<float*>(escr) + row * (BN + 1);
     int it = 0, t = 0;
     uint32_t uses = 0;  // EG = 2: chunks drained from this group's buffer so far
     bool ok = true;
     for (int it_ = blockIdx.x; it_ < tiles && ok; it_ += gridDim.x, ++t) {
       if (EG > 1 && (t % EG) != eg) continue;
-      const int tile = S.reverse ? tiles - 1 - it_ : it_;
-      const int nti = tile % S.nt, rest = tile / S.nt;
-      const int mti = rest % S.mt, z = rest / S.mt;
-      const int k0 = (z % S.ksplit) * S.kchunk;
-      const int KB = (min(S.kchunk, S.K - k0) + kUBK - 1) / kUBK;
+      int local;
+      const UmmaParams<Epi>& P = src.entry(it_, local);
+      const UmmaShape& S = P.s;
+      const TileAt tl = locate(S, local);
+      const int KB = tl.KB;
       const int kc = S.kc > 0 ? S.kc : KB;
       const int nch = (KB + kc - 1) / kc;
       for (int ch = 0; ch < nch; ++ch, ++it) {
         const int buf = EG > 1 ? eg : (it & 1);
         const uint32_t use = EG > 1 ? uses++ : (uint32_t)(it >> 1);
-        if (!mbar_wait_abortable(&accf[buf], use & 1, abort_s)) { fail(); ok = false; break; }
+        if (!mbar_wait_abortable(&accf[buf], use & 1, abort_s)) { fail(S.err); ok = false; break; }
         tc_fence_after();
         const uint32_t taddr = tbase + ((uint32_t)(sub * 32) << 16) + buf * acc_stride;
         if (nch == 1) {
           // z = batch * ksplit + split
-          P.epi.template tile<BN>(z, mti, nti, row, AccSrc{taddr, S.ngroups, BN, nullptr}, S,
+          P.epi.template tile<BN>(tl.z, tl.mti, tl.nti, row, AccSrc{taddr, ngrp, BN, nullptr}, S,
                                   escr);
           tc_fence_before();
           __syncwarp();
@@ -262,7 +330,7 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
 #pragma unroll 1
           for (int c = 0; c < BN / 16; ++c) {
             float v[16];
-            acc_ld16(taddr + c * 16, S.ngroups, BN, v);
+            acc_ld16(taddr + c * 16, ngrp, BN, v);
 #pragma unroll
             for (int i = 0; i < 16; ++i)
               srow[c * 16 + i] = (ch == 0) ? v[i] : srow[c * 16 + i] + v[i];
@@ -271,7 +339,7 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive(&acce[buf]);
           if (ch == nch - 1)
-            P.epi.template tile<BN>(z, mti, nti, row, AccSrc{0u, 1, BN, srow}, S, escr);
+            P.epi.template tile<BN>(tl.z, tl.mti, tl.nti, row, AccSrc{0u, 1, BN, srow}, S, escr);
         }
       }
     }
@@ -282,6 +350,18 @@ __global__ void __launch_bounds__(64 + 128 * EG, 1)
     tc_fence_after();
     tmem_dealloc(tbase, kCols);
   }
+}
+
+template <int BN, class Epi, int EG>
+__global__ void __launch_bounds__(64 + 128 * EG, 1)
+    umma_gemm_kernel(const __grid_constant__ UmmaParams<Epi> P) {
+  umma_body<BN, Epi, EG>(UmmaOne<Epi>{P});
+}
+
+template <int BN, class Epi, int EG>
+__global__ void __launch_bounds__(64 + 128 * EG, 1)
+    umma_group_kernel(const __grid_constant__ UmmaGroup<Epi> G) {
+  umma_body<BN, Epi, EG>(UmmaMany<Epi>{G});
 }
 
 // ---------------------------------------------------------------------------
@@ -305,6 +385,24 @@ cudaError_t launch_umma(const UmmaParams<Epi>& P, int num_sms, cudaStream_t st) 
   const int tiles = P.s.batch * P.s.ksplit * P.s.mt * P.s.nt;
   const int grid = tiles < num_sms ? tiles : num_sms;
   umma_gemm_kernel<BN, Epi, EG><<<grid, 64 + 128 * EG, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+// A group of GEMMs in one launch.  `shape0` is any entry's shape (host copy):
+// pieces, accumulator groups and epilogue scratch are the same for all.
+template <int BN, int EG = 1, class Epi>
+cudaError_t launch_umma_group(const UmmaGroup<Epi>& G, const UmmaShape& shape0, int num_sms,
+                              cudaStream_t st) {
+  const size_t smem = umma_smem_bytes(BN, G.stages, shape0.npa, shape0.npb, size_t(EG) * shape0.epi_bytes);
+  if (G.n < 1 || G.n > kUmmaMaxGroup || G.stages < 2 || smem > kUmmaSmemBudget ||
+      (shape0.epi_bytes & 255) || (EG > 2 ? EG : 2) * shape0.ngroups * BN > 512)
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(umma_group_kernel<BN, Epi, EG>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int tiles = G.start[G.n];
+  const int grid = tiles < num_sms ? tiles : num_sms;
+  umma_group_kernel<BN, Epi, EG><<<grid, 64 + 128 * EG, smem, st>>>(G);
   return cudaGetLastError();
 }
 

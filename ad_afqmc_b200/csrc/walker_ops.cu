@@ -17,9 +17,8 @@ namespace {
 // ---------------------------------------------------------------------------
 constexpr int kWeightThreads = 1024;
 
-__global__ void __launch_bounds__(kWeightThreads)
-    weight_kernel(int W, double dt, const double* scal, const double* wscal, double* weights,
-                  double* overlaps, double* scalars) {
+__device__ __forceinline__ void weight_body(int W, double dt, const double* scal, const double* wscal,
+                                            double* weights, double* overlaps, double* scalars) {
   __shared__ double red[kWeightThreads / 32];
   const double sdt = sqrt(dt);
   const double h0r = scal[1], h0i = scal[2];
@@ -56,6 +55,18 @@ __global__ void __launch_bounds__(kWeightThreads)
   }
   tot = block_sum(tot, red);
   if (threadIdx.x == 0) scalars[1] = est - 0.1 * log(tot / W) / dt;
+}
+
+__global__ void __launch_bounds__(kWeightThreads)
+    weight_kernel(int W, double dt, const double* scal, const double* wscal, double* weights,
+                  double* overlaps, double* scalars) {
+  weight_body(W, dt, scal, wscal, weights, overlaps, scalars);
+}
+
+// one CTA per solve of a batch
+__global__ void __launch_bounds__(kWeightThreads) weight_kernel_grouped(const WeightArgs* A) {
+  const WeightArgs& a = A[blockIdx.x];
+  weight_body(a.W, a.dt, a.scal, a.wscal, a.weights, a.overlaps, a.scalars);
 }
 
 // ---------------------------------------------------------------------------
@@ -397,6 +408,12 @@ cudaError_t launch_weight_update(const Layout& L, const double* prep, double* wo
   ProfScope ps(K_WEIGHT, st);
   weight_kernel<<<1, kWeightThreads, 0, st>>>(L.W, dt, prep + L.p_scal, work + L.w_wscal, weights,
                                               overlaps, scalars);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_weight_grouped(const WeightArgs* args, int n, cudaStream_t st) {
+  ProfScope ps(K_WEIGHT, st);
+  weight_kernel_grouped<<<n, kWeightThreads, 0, st>>>(args);
   return cudaGetLastError();
 }
 

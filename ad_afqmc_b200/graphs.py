@@ -89,22 +89,41 @@ class BlockGraph:
 
     # -- the recorded body ---------------------------------------------------
     def body(self) -> None:
+        n0 = _lib.launch_count()
+        st = self.body_begin()
+        self.body_steps(st)
+        self.body_end(st)
+        self.launches_per_block = _lib.launch_count() - n0
+
+    def body_begin(self) -> _lib.afq_state:
+        """The block's prologue: population shift, killed count, fields."""
         lib = _lib.lib()
         stream = _lib.stream_handle()
-        pd, eng = self.pd, self.eng
-        sc = pd["_scalars"]
+        sc = self.pd["_scalars"]
         sc[1].copy_(sc[0])  # pop_control_ene_shift = e_estimate
         sc[2].zero_()       # n_killed_walkers
-        n0 = _lib.launch_count()
         if not self.external_fields:
             _lib.check(lib.afq_normal_fields_dev(self.fields.data_ptr(), self.fields.numel(), self.seed,
                                                  self.counter.data_ptr(), stream), "afq_normal_fields_dev")
-        st = make_state(pd)  # GREEN_CURRENT clear: the first step computes G
+        return make_state(self.pd)  # GREEN_CURRENT clear: the first step computes G
+
+    def body_steps(self, st: _lib.afq_state) -> None:
+        lib = _lib.lib()
+        stream = _lib.stream_handle()
+        eng = self.eng
         p, w, wb = eng.handle
         for s in range(self.S):
             _lib.check(lib.afq_propagate_constrained(C.byref(eng.dims), p, C.byref(st),
                                                      self.fields[s].data_ptr(), w, wb, stream),
                        "afq_propagate_constrained")
+
+    def body_end(self, st: _lib.afq_state) -> None:
+        """Block end, reconfiguration, overlaps, e_estimate, status."""
+        lib = _lib.lib()
+        stream = _lib.stream_handle()
+        pd, eng = self.pd, self.eng
+        sc = pd["_scalars"]
+        p, w, wb = eng.handle
         if self.lno:
             self._lno_block_end(lib, stream)
         else:
@@ -115,7 +134,6 @@ class BlockGraph:
             if self.update_estimate:
                 sc[0].mul_(0.9).add_(0.1 * self.block_out[0])
             self._fold_status()
-            self.launches_per_block = _lib.launch_count() - n0
             pd.pop("_afq_green_of", None)
             return
         _lib.check(lib.afq_uniform_dev(self.zeta.data_ptr(), self.seed, self.counter.data_ptr(), stream),
@@ -136,7 +154,6 @@ class BlockGraph:
         if self.update_estimate:
             sc[0].mul_(0.9).add_(0.1 * self.block_out[0])
         self._fold_status()
-        self.launches_per_block = _lib.launch_count() - n0
         pd.pop("_afq_green_of", None)
 
     def _fold_status(self) -> None:
@@ -257,6 +274,107 @@ class BatchGraph:
     @property
     def launches_per_block(self) -> int:
         return sum(b.launches_per_block for b in self.blocks)
+
+
+class GroupedBatchGraph:
+    """Blocks of many independent mixed-precision solves in one graph, with
+    the phaseless steps of all solves in grouped launches (afq_batch_*): per
+    step each kernel family runs once for the whole batch, the force-bias,
+    VHS and propagator contractions as persistent grouped tcgen05 kernels over
+    (solve, tile) work lists.  The per-solve block prologue (fields) and block
+    end (QR, energies, comb) run on forked streams as in ``BatchGraph``.  Each
+    solve's results equal its own ``BlockGraph`` replays bit for bit.  At most
+    64 solves (afq_batch limit); all with the same steps per block and Taylor
+    terms."""
+
+    def __init__(self, blocks: List[BlockGraph], n_streams: int = 16):
+        if not 1 <= len(blocks) <= 64:
+            raise _lib.AfqError("a grouped batch holds 1 to 64 solves")
+        S = blocks[0].S
+        for b in blocks:
+            if b.S != S or b.external_fields or b.lno:
+                raise _lib.AfqError("grouped batches need equal steps per block, device fields, no LNO")
+            b.eng.ensure_workspace()
+        self.blocks = blocks
+        self.S = S
+        self.n_streams = max(1, min(n_streams, len(blocks)))
+        n = len(blocks)
+        lib = _lib.lib()
+        self._dims = (_lib.afq_dims * n)(*[b.eng.dims for b in blocks])
+        self._prep = (C.c_void_p * n)(*[b.eng.prepared.data_ptr() for b in blocks])
+        self._work = (C.c_void_p * n)(*[b.eng.work.data_ptr() for b in blocks])
+        self._wbytes = (C.c_size_t * n)(*[b.eng.work_bytes for b in blocks])
+        self._states = (_lib.afq_state * n)(*[make_state(b.pd) for b in blocks])
+        self._fields = (C.c_void_p * n)(*[b.fields.data_ptr() for b in blocks])
+        size = C.c_size_t()
+        _lib.check(lib.afq_batch_table_size(n, C.cast(self._dims, C.c_void_p), C.byref(size)),
+                   "afq_batch_table_size")
+        dev = blocks[0].fields.device
+        self.table = torch.empty((size.value + 511) // 8 + 64, dtype=torch.float64, device=dev)
+        base = (self.table.data_ptr() + 255) & ~255
+        self._handle = C.c_void_p()
+        torch.cuda.synchronize()
+        _lib.check(lib.afq_batch_create(n, C.cast(self._dims, C.c_void_p), C.cast(self._prep, C.c_void_p),
+                                        C.cast(self._work, C.c_void_p), C.cast(self._wbytes, C.c_void_p),
+                                        C.cast(self._states, C.c_void_p), C.cast(self._fields, C.c_void_p),
+                                        base, size.value, C.byref(self._handle)), "afq_batch_create")
+        self.graph: Optional[torch.cuda.CUDAGraph] = None
+        self.launches_per_block = 0
+
+    def _record(self):
+        lib = _lib.lib()
+        n0 = _lib.launch_count()
+        main = torch.cuda.current_stream()
+        streams = [torch.cuda.Stream() for _ in range(self.n_streams)]
+        for s in streams:
+            s.wait_stream(main)
+        states = []
+        for i, b in enumerate(self.blocks):
+            with torch.cuda.stream(streams[i % self.n_streams]):
+                states.append(b.body_begin())
+        for s in streams:
+            main.wait_stream(s)
+        for step in range(self.S):
+            _lib.check(lib.afq_batch_propagate_constrained(self._handle, step, 1 if step > 0 else 0,
+                                                           _lib.stream_handle(main)),
+                       "afq_batch_propagate_constrained")
+        for s in streams:
+            s.wait_stream(main)
+        for i, b in enumerate(self.blocks):
+            with torch.cuda.stream(streams[i % self.n_streams]):
+                b.body_end(states[i])
+        for s in streams:
+            main.wait_stream(s)
+        self.launches_per_block = _lib.launch_count() - n0
+
+    def body(self) -> None:
+        """One block, launched eagerly (no graph)."""
+        self._record()
+
+    def capture(self, warmup: int = 1) -> "GroupedBatchGraph":
+        for _ in range(warmup):
+            self._record()
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._record()
+        return self
+
+    def replay(self) -> None:
+        self.graph.replay()
+
+    def check_status(self) -> None:
+        for b in self.blocks:
+            b.check_status()
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().afq_batch_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
 
 
 class HostFieldBlocks:

@@ -298,6 +298,30 @@ typedef struct afq_tuning {
 int afq_set_tuning(const afq_dims* d, const afq_tuning* t);
 int afq_get_tuning(const afq_dims* d, afq_tuning* out);
 
+/* ---- Batches of independent solves (uneven fragments) ---------------------
+ * No counterpart in the reference, which solves LNO fragments one process at
+ * a time (lnoutils.py:175-177).  A batch advances up to 64 solves of
+ * different sizes (each with its own afq_dims, prepared buffer, workspace and
+ * afq_state, all precision AFQ_MIXED or AFQ_MIXED_HI with the same
+ * n_exp_terms) one phaseless step at a time: every kernel of the step runs
+ * ONCE for the whole batch over a device table of per-solve arguments, and
+ * the force-bias, VHS and propagator contractions run as persistent grouped
+ * tcgen05 kernels over (solve, tile) work lists, one launch per tile shape.
+ * Each solve gets the arithmetic of its own afq_propagate_constrained call,
+ * bit for bit.  The table is caller-owned device memory of
+ * afq_batch_table_size() bytes (256-byte aligned), written once by
+ * afq_batch_create (synchronously); the buffers it points to must stay put.
+ * fields[f]: solve f's fields of step 0, (W_f, G_f) float64; step s reads
+ * fields[f] + s * W_f * G_f.  green_current: the workspaces hold the Green's
+ * functions of the current walkers (every step of a block but the first). */
+typedef struct afq_batch afq_batch;
+int afq_batch_table_size(int32_t n, const afq_dims* dims, size_t* bytes);
+int afq_batch_create(int32_t n, const afq_dims* dims, const void* const* prepared, void* const* work,
+                     const size_t* work_bytes, const afq_state* states, const double* const* fields,
+                     void* table, size_t table_bytes, afq_batch** out);
+int afq_batch_propagate_constrained(afq_batch* b, int32_t step, int32_t green_current, void* stream);
+int afq_batch_destroy(afq_batch* b);
+
 /* ---- Per-solve Hamiltonian intermediates (FP64, device pointers) ----------
  * These replace the set-up half of the walker path, run once per solve:
  * every contraction runs on the FP64 tensor cores of this library.  They
