@@ -10,7 +10,9 @@
 //                (wave_function.get_init_walkers, wavefunctions.py:427-466)
 //
 // The contractions run on the FP64 tensor cores through the same DMMA main
-// loop as the walker kernels (gemm_f64.cuh).  v0 is a split-K GEMM over the
+// loop as the walker kernels (gemm_f64.cuh), which copies 16-byte pieces:
+// every operand it reads has an even leading dimension (odd N: the Cholesky
+// vectors and square matrices are first copied to padded rows).  v0 is a split-K GEMM over the
 // Cholesky index with partial sums added in a fixed order, so results do not
 // depend on the device.  The matrix exponential is scaling and squaring of
 // a truncated Taylor series (Moler and Van Loan, "Nineteen dubious ways to
@@ -94,19 +96,42 @@ cudaError_t dgemm(const DgemmArgs& a, int zdim, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// plain square product C = alpha A B (+ diag I), n x n row-major, ld n
-cudaError_t square_gemm(int n, const double* A, const double* B, double alpha, double diag, double* C,
-                        cudaStream_t st) {
+// plain square product C = alpha A B (+ diag I), n x n row-major, all with the
+// (even) row stride ld
+cudaError_t square_gemm(int n, long long ld, const double* A, const double* B, double alpha,
+                        double diag, double* C, cudaStream_t st) {
   DgemmArgs a{};
-  a.A = F64Operand{A, n, 0, 0, kUnsegS};
-  a.B = F64Operand{B, n, 0, 0, kUnsegS};
+  a.A = F64Operand{A, ld, 0, 0, kUnsegS};
+  a.B = F64Operand{B, ld, 0, 0, kUnsegS};
   a.M = a.N = a.K = n;
   a.nbatch = 1;
   a.alpha = alpha;
   a.diag = diag;
   a.C = C;
-  a.ldc = n;
+  a.ldc = ld;
   return dgemm<CfgS>(a, 1, st);
+}
+
+// dst[r * ldd + c] = src[r * lds + c] for r < rows, c < cols
+__global__ void copy2d_kernel(long long rows, int cols, const double* src, long long lds, double* dst,
+                              long long ldd) {
+  const long long n = rows * cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / cols;
+    const int c = (int)(e - r * cols);
+    dst[r * ldd + c] = src[r * lds + c];
+  }
+}
+
+cudaError_t copy2d(long long rows, int cols, const double* src, long long lds, double* dst,
+                   long long ldd, cudaStream_t st) {
+  long long blocks = (rows * cols + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  ProfScope ps(K_MISC, st);
+  copy2d_kernel<<<(int)blocks, 256, 0, st>>>(rows, cols, src, lds, dst, ldd);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -114,8 +139,8 @@ cudaError_t square_gemm(int n, const double* A, const double* B, double alpha, d
 // ---------------------------------------------------------------------------
 // h1[s] <- (h1[s] + h1[s]^T)/2 in place for both spins; hrot[0] = RHF: (h1[0]+h1[1])/2,
 // UHF: h1[0]; hrot[1] = h1[1] (UHF only); mot[s] = mo[s]^T (no x N)
-__global__ void sym_kernel(int n, double* h1, double* hrot, int uhf) {
-  const long long nn = (long long)n * n;
+__global__ void sym_kernel(int n, double* h1, double* hrot, long long ldh, int uhf) {
+  const long long nn = (long long)n * n, hs = (long long)n * ldh;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
        e += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(e / n), j = (int)(e % n);
@@ -130,23 +155,24 @@ __global__ void sym_kernel(int n, double* h1, double* hrot, int uhf) {
     }
     if (uhf) {
       for (int s = 0; s < 2; ++s) {
-        hrot[s * nn + (long long)i * n + j] = a[s];
-        hrot[s * nn + (long long)j * n + i] = a[s];
+        hrot[s * hs + (long long)i * ldh + j] = a[s];
+        hrot[s * hs + (long long)j * ldh + i] = a[s];
       }
     } else {
       const double v = 0.5 * (a[0] + a[1]);
-      hrot[(long long)i * n + j] = v;
-      hrot[(long long)j * n + i] = v;
+      hrot[(long long)i * ldh + j] = v;
+      hrot[(long long)j * ldh + i] = v;
     }
   }
 }
 
-__global__ void transpose_kernel(int rows, int cols, const double* in, double* out) {
+// out (cols x rows, row stride ldo) = in (rows x cols)^T
+__global__ void transpose_kernel(int rows, int cols, const double* in, double* out, long long ldo) {
   const long long nn = (long long)rows * cols;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
        e += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(e / cols), c = (int)(e % cols);
-    out[(long long)c * rows + r] = in[e];
+    out[(long long)c * ldo + r] = in[e];
   }
 }
 
@@ -215,12 +241,12 @@ __global__ void hmod_kernel(long long nn, int np, const double* h1, int avg, con
 // matrix exponential helpers
 // ---------------------------------------------------------------------------
 // ||A||_1 (largest column sum of |a_ij|), one CTA
-__global__ void __launch_bounds__(256) norm1_kernel(int n, const double* A, double* out) {
+__global__ void __launch_bounds__(256) norm1_kernel(int n, const double* A, long long lda, double* out) {
   __shared__ double red[256];
   double m = 0.0;
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
     double s = 0.0;
-    for (int i = 0; i < n; ++i) s += fabs(A[(long long)i * n + j]);
+    for (int i = 0; i < n; ++i) s += fabs(A[(long long)i * lda + j]);
     m = fmax(m, s);
   }
   red[threadIdx.x] = m;
@@ -232,13 +258,13 @@ __global__ void __launch_bounds__(256) norm1_kernel(int n, const double* A, doub
   if (threadIdx.x == 0) *out = red[0];
 }
 
-// P = I + B / m  (the innermost Horner factor)
-__global__ void horner_init_kernel(int n, const double* B, double inv_m, double* P) {
+// P = I + B / m  (the innermost Horner factor); both with row stride ld
+__global__ void horner_init_kernel(int n, long long ld, const double* B, double inv_m, double* P) {
   const long long nn = (long long)n * n;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
        e += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(e / n), j = (int)(e % n);
-    P[e] = B[e] * inv_m + (i == j ? 1.0 : 0.0);
+    P[i * ld + j] = B[i * ld + j] * inv_m + (i == j ? 1.0 : 0.0);
   }
 }
 
@@ -248,6 +274,7 @@ __global__ void horner_init_kernel(int n, const double* B, double inv_m, double*
 constexpr int kJacobiThreads = 1024;
 constexpr int kJacobiMaxSweeps = 40;
 constexpr int kJacobiMaxN = 2048;
+constexpr int kJacobiSmemN = 160;  // matrix in shared memory up to this order
 
 // round-robin pairing: position k of round r (n even, positions 0..n-1)
 __device__ __forceinline__ int rr_index(int k, int r, int n) {
@@ -255,36 +282,43 @@ __device__ __forceinline__ int rr_index(int k, int r, int n) {
   return 1 + (k - 1 + r) % (n - 1);
 }
 
-// A (n x n, ld n, symmetric) is overwritten; V (n x n) receives the
-// eigenvectors as columns; evals/evecs: sorted descending.  n_pad = n rounded
-// up to even; the padding index (n) is a phantom with no rotations.
-__global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(int n, double* A, double* V,
-                                                                double* evals, double* evecs,
-                                                                int* sweeps_out) {
-  extern __shared__ double js[];
+// A (n x n, row stride lda, symmetric; shared or global memory) is
+// overwritten; V (global, n x n) receives the eigenvectors as columns;
+// evals/evecs: sorted descending.  One round applies the npair disjoint
+// rotations of the round-robin ordering at once: the 2x2 block of A on rows
+// {p1, q1} and columns {p2, q2} becomes J1^T A J2 (J = [[c, s], [-s, c]] on
+// (p, q)), and the rotated pair's own off-diagonal element is set to zero.
+// The padding index n (odd n) is a phantom without rotations.  Sweeps stop
+// when the off-diagonal Frobenius norm is at most 4 n eps of the matrix's.
+__device__ void jacobi_body(int n, double* A, long long lda, double* V, double* evals, double* evecs,
+                            int* sweeps_out, double* cs, double* sn, int* pp, int* qq) {
+  __shared__ double red[32];
   const int np = (n + 1) & ~1;
   const int npair = np / 2;
-  double* cs = js;                 // [npair] c
-  double* sn = cs + npair;         // [npair] s
-  int* pp = reinterpret_cast<int*>(sn + npair);  // [npair] p
-  int* qq = pp + npair;                           // [npair] q
-  __shared__ double red[32];
   const int tid = threadIdx.x, nt = blockDim.x;
-  const long long nn = (long long)n * n;
-  for (long long e = tid; e < nn; e += nt) V[e] = ((e / n) == (e % n)) ? 1.0 : 0.0;
+  for (int e = tid; e < n * n; e += nt) V[e] = ((e / n) == (e % n)) ? 1.0 : 0.0;
   double fro = 0.0;
-  for (long long e = tid; e < nn; e += nt) fro += A[e] * A[e];
+  for (int e = tid; e < n * n; e += nt) {
+    const double x = A[(long long)(e / n) * lda + e % n];
+    fro += x * x;
+  }
   fro = block_sum(fro, red);
-  const double tol2 = fro * 1e-30;
+  const double eps = 2.220446049250313e-16;
+  const double tol2 = fro * (4.0 * n * eps) * (4.0 * n * eps);
   int sweep = 0;
   for (; sweep < kJacobiMaxSweeps; ++sweep) {
     double off = 0.0;
-    for (long long e = tid; e < nn; e += nt)
-      if ((e / n) != (e % n)) off += A[e] * A[e];
+    for (int e = tid; e < n * n; e += nt) {
+      const int i = e / n, j = e - i * n;
+      if (i != j) {
+        const double x = A[(long long)i * lda + j];
+        off += x * x;
+      }
+    }
     off = block_sum(off, red);
     if (off <= tol2 || fro == 0.0) break;
     for (int r = 0; r < np - 1; ++r) {
-      // rotation parameters of this round (GVL Algorithm 8.5.1, sym.schur2)
+      // rotation parameters (Golub & Van Loan, Algorithm 8.5.1, sym.schur2)
       for (int k = tid; k < npair; k += nt) {
         int p = rr_index(k, r, np), q = rr_index(np - 1 - k, r, np);
         if (p > q) {
@@ -294,9 +328,9 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(int n, double* A
         }
         double c = 1.0, s = 0.0;
         if (q < n) {
-          const double apq = A[(long long)p * n + q];
-          const double app = A[(long long)p * n + p], aqq = A[(long long)q * n + q];
-          if (apq != 0.0 && fabs(apq) > 1e-300) {
+          const double apq = A[(long long)p * lda + q];
+          if (apq != 0.0) {
+            const double app = A[(long long)p * lda + p], aqq = A[(long long)q * lda + q];
             const double tau = (aqq - app) / (2.0 * apq);
             const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
             c = 1.0 / sqrt(1.0 + t * t);
@@ -309,55 +343,78 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(int n, double* A
         qq[k] = q < n ? q : -1;
       }
       __syncthreads();
-      // columns: A <- A J, V <- V J
-      for (long long it = tid; it < (long long)npair * n; it += nt) {
-        const int k = (int)(it / n), i = (int)(it % n);
+      // A <- J^T A J, one 2x2 block per (k1, k2)
+      for (int it = tid; it < npair * npair; it += nt) {
+        const int k1 = it / npair, k2 = it - k1 * npair;
+        const int p1 = pp[k1], q1 = qq[k1], p2 = pp[k2], q2 = qq[k2];
+        const double c1 = cs[k1], s1 = sn[k1], c2 = cs[k2], s2 = sn[k2];
+        if (s1 == 0.0 && s2 == 0.0) continue;
+        double* rp = A + (long long)p1 * lda;
+        double* rq = q1 >= 0 ? A + (long long)q1 * lda : nullptr;
+        const double x00 = rp[p2], x01 = q2 >= 0 ? rp[q2] : 0.0;
+        const double x10 = rq ? rq[p2] : 0.0, x11 = (rq && q2 >= 0) ? rq[q2] : 0.0;
+        // columns: [y0 y1] = [x0 x1] J2
+        const double a00 = c2 * x00 - s2 * x01, a01 = s2 * x00 + c2 * x01;
+        const double a10 = c2 * x10 - s2 * x11, a11 = s2 * x10 + c2 * x11;
+        // rows: J1^T
+        double b00 = c1 * a00 - s1 * a10, b01 = c1 * a01 - s1 * a11;
+        double b10 = s1 * a00 + c1 * a10, b11 = s1 * a01 + c1 * a11;
+        if (k1 == k2 && s1 != 0.0) {
+          b01 = 0.0;
+          b10 = 0.0;
+        }
+        rp[p2] = b00;
+        if (q2 >= 0) rp[q2] = b01;
+        if (rq) {
+          rq[p2] = b10;
+          if (q2 >= 0) rq[q2] = b11;
+        }
+      }
+      // V <- V J
+      for (int it = tid; it < npair * n; it += nt) {
+        const int k = it / n, i = it - k * n;
         const int p = pp[k], q = qq[k];
-        if (q < 0 || sn[k] == 0.0) continue;
         const double c = cs[k], s = sn[k];
-        double* ar = A + (long long)i * n;
-        const double x = ar[p], y = ar[q];
-        ar[p] = c * x - s * y;
-        ar[q] = s * x + c * y;
+        if (q < 0 || s == 0.0) continue;
         double* vr = V + (long long)i * n;
         const double u = vr[p], w = vr[q];
         vr[p] = c * u - s * w;
         vr[q] = s * u + c * w;
       }
       __syncthreads();
-      // rows: A <- J^T A
-      for (long long it = tid; it < (long long)npair * n; it += nt) {
-        const int k = (int)(it / n), j = (int)(it % n);
-        const int p = pp[k], q = qq[k];
-        if (q < 0 || sn[k] == 0.0) continue;
-        const double c = cs[k], s = sn[k];
-        const double x = A[(long long)p * n + j], y = A[(long long)q * n + j];
-        A[(long long)p * n + j] = c * x - s * y;
-        A[(long long)q * n + j] = s * x + c * y;
-      }
-      __syncthreads();
-      // the rotated pair's off-diagonal element is zero by construction
-      for (int k = tid; k < npair; k += nt) {
-        const int p = pp[k], q = qq[k];
-        if (q < 0 || sn[k] == 0.0) continue;
-        A[(long long)p * n + q] = 0.0;
-        A[(long long)q * n + p] = 0.0;
-      }
-      __syncthreads();
     }
   }
   // descending order: rank of eigenvalue i (ties by index)
   for (int i = tid; i < n; i += nt) {
-    const double li = A[(long long)i * n + i];
+    const double li = A[(long long)i * lda + i];
     int rank = 0;
     for (int j = 0; j < n; ++j) {
-      const double lj = A[(long long)j * n + j];
+      const double lj = A[(long long)j * lda + j];
       if (lj > li || (lj == li && j < i)) ++rank;
     }
     evals[rank] = li;
     for (int row = 0; row < n; ++row) evecs[(long long)row * n + rank] = V[(long long)row * n + i];
   }
   if (tid == 0 && sweeps_out) *sweeps_out = sweep;
+}
+
+// A: the input matrix (n x n, ld n, global, read only); Ag: global scratch
+// (n x n) used when the matrix does not fit shared memory
+__global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(int n, const double* A, double* Ag,
+                                                                double* V, double* evals,
+                                                                double* evecs, int* sweeps_out) {
+  extern __shared__ double js[];
+  const int npair = ((n + 1) & ~1) / 2;
+  double* cs = js;
+  double* sn = cs + npair;
+  int* pp = reinterpret_cast<int*>(sn + npair);
+  int* qq = pp + npair;
+  double* As = reinterpret_cast<double*>(qq + npair);  // 24 npair bytes in: 8-byte aligned
+  const bool in_smem = n <= kJacobiSmemN;
+  double* M = in_smem ? As : Ag;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) M[e] = A[e];
+  __syncthreads();
+  jacobi_body(n, M, n, V, evals, evecs, sweeps_out, cs, sn, pp, qq);
 }
 
 int vsplits(int n, int G, int* bsum) {
@@ -372,6 +429,12 @@ int vsplits(int n, int G, int* bsum) {
 
 constexpr int kV1Split = 16;
 
+// doubles of afq_expm's scratch: padded A, two Horner/squaring buffers, the norm
+long long expm_work(int n) {
+  const long long ld = even(n);
+  return 3 * (long long)n * ld + 8;
+}
+
 }  // namespace
 }  // namespace afq
 
@@ -382,12 +445,15 @@ extern "C" {
 int afq_intermediates_workspace_size(int32_t norb, int32_t nchol, size_t* bytes) {
   if (!bytes) return AFQ_ERR_NULL;
   if (norb <= 0 || nchol <= 0 || norb > kJacobiMaxN) return AFQ_ERR_SHAPE;
-  const long long nn = (long long)norb * norb;
+  const long long nn = (long long)norb * norb, ld = even(norb);
   int bsum = 0;
   const int nz = vsplits(norb, nchol, &bsum);
-  // v0 partials, v1 partials, hmod (2 spins), three expm buffers, the norm, eigensolver copy + V
-  long long d = nz * nn + (long long)kV1Split * nn + 2 * nn + 3 * nn + 2 + 2 * nn + 8;
-  d += 64;  // alignment slack between sub-buffers
+  // v0 partials, v1 partials, h1_mod (2 spins), the exponential's scratch, and
+  // (odd N) the Cholesky vectors with padded rows; the measurement set-up uses
+  // the front of the same space
+  long long d = even(nz * nn) + even((long long)kV1Split * nn) + even(2 * nn) + expm_work(norb);
+  if (norb & 1) d += (long long)nchol * norb * ld;
+  d += 64;
   *bytes = (size_t)d * sizeof(double);
   return AFQ_OK;
 }
@@ -405,31 +471,38 @@ int afq_measurement_intermediates(int32_t norb, const int32_t nocc[2], int32_t n
     if (!mo[s] || !rot_h1[s] || !rot_chol[s]) return AFQ_ERR_NULL;
   }
   size_t need = 0;
-  afq_intermediates_workspace_size(norb, nchol, &need);
+  const int rc0 = afq_intermediates_workspace_size(norb, nchol, &need);
+  if (rc0 != AFQ_OK) return rc0;
   if (work_bytes < need) return AFQ_ERR_WORKSPACE;
-  if (!al16(work)) return AFQ_ERR_ALIGN;
+  if (!al16(work) || !al16(chol)) return AFQ_ERR_ALIGN;
   cudaStream_t st = as_stream(stream);
   const int n = norb;
-  const long long nn = (long long)n * n;
-  double* hrot = static_cast<double*>(work);  // 2 nn
-  double* mot = hrot + even(2 * nn);          // no x n per spin (<= nn each)
+  const long long ld = even(n), hs = (long long)n * ld;
+  double* hrot = static_cast<double*>(work);  // 2 spins, row stride ld
+  double* mot = hrot + 2 * hs;                // no x n per spin, row stride ld
+  double* cholp = mot + 2 * hs;               // odd n: chol with padded rows
+  const double* B = chol;
+  if (n & 1) {
+    if (copy2d((long long)nchol * n, n, chol, n, cholp, ld, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    B = cholp;
+  }
   {
     ProfScope ps(K_MISC, st);
-    sym_kernel<<<(int)((nn + 255) / 256), 256, 0, st>>>(n, h1, hrot, ns == 2);
+    sym_kernel<<<(int)((hs + 255) / 256), 256, 0, st>>>(n, h1, hrot, ld, ns == 2);
     if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
   }
   for (int s = 0; s < ns; ++s) {
     const int no = nocc[s];
-    double* mt = mot + s * even(nn);
+    double* mt = mot + s * hs;
     {
       ProfScope ps(K_MISC, st);
-      transpose_kernel<<<(int)(((long long)n * no + 255) / 256), 256, 0, st>>>(n, no, mo[s], mt);
+      transpose_kernel<<<(int)(((long long)n * no + 255) / 256), 256, 0, st>>>(n, no, mo[s], mt, ld);
       if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
     }
     // rot_h1[s] = mo^T h (no x n)
     DgemmArgs a{};
-    a.A = F64Operand{mt, n, 0, 0, kUnsegS};
-    a.B = F64Operand{hrot + s * nn, n, 0, 0, kUnsegS};
+    a.A = F64Operand{mt, ld, 0, 0, kUnsegS};
+    a.B = F64Operand{hrot + s * hs, ld, 0, 0, kUnsegS};
     a.M = no;
     a.N = n;
     a.K = n;
@@ -440,8 +513,8 @@ int afq_measurement_intermediates(int32_t norb, const int32_t nocc[2], int32_t n
     if (dgemm<CfgS>(a, 1, st) != cudaSuccess) return AFQ_ERR_CUDA;
     // rot_chol[s][g] = mo^T L_g (no x n), batched over g
     DgemmArgs b{};
-    b.A = F64Operand{mt, n, 0, 0, kUnsegS};
-    b.B = F64Operand{chol, n, nn, 0, kUnsegS};
+    b.A = F64Operand{mt, ld, 0, 0, kUnsegS};
+    b.B = F64Operand{B, ld, (long long)n * ld, 0, kUnsegS};
     b.M = no;
     b.N = n;
     b.K = n;
@@ -459,18 +532,20 @@ int afq_expm(int32_t n, const double* A, double scale, double* out, void* work, 
              void* stream) {
   if (!A || !out || !work) return AFQ_ERR_NULL;
   if (n <= 0 || n > kJacobiMaxN) return AFQ_ERR_SHAPE;
-  const long long nn = (long long)n * n;
-  if (work_bytes < (size_t)(2 * even(nn) + 2) * sizeof(double)) return AFQ_ERR_WORKSPACE;
+  if (work_bytes < (size_t)expm_work(n) * sizeof(double)) return AFQ_ERR_WORKSPACE;
   if (!al16(work)) return AFQ_ERR_ALIGN;
   if (out == A) return AFQ_ERR_ARG;
   cudaStream_t st = as_stream(stream);
-  double* P = static_cast<double*>(work);
-  double* Q = P + even(nn);
-  double* nrm = Q + even(nn);
-  const int blocks = (int)((nn + 255) / 256);
+  const long long ld = even(n), ms = (long long)n * ld;
+  double* Ap = static_cast<double*>(work);  // A with padded rows
+  double* P = Ap + ms;
+  double* Q = P + ms;
+  double* nrm = Q + ms;
+  const int blocks = (int)(((long long)n * n + 255) / 256);
+  if (copy2d(n, n, A, n, Ap, ld, st) != cudaSuccess) return AFQ_ERR_CUDA;
   {
     ProfScope ps(K_MISC, st);
-    norm1_kernel<<<1, 256, 0, st>>>(n, A, nrm);
+    norm1_kernel<<<1, 256, 0, st>>>(n, Ap, ld, nrm);
     if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
   }
   double theta0 = 0.0;
@@ -495,30 +570,25 @@ int afq_expm(int32_t n, const double* A, double scale, double* out, void* work, 
   // Horner: P = I + B/m ; P <- I + B P / k for k = m-1 .. 1 ; B = bscale A
   {
     ProfScope ps(K_MISC, st);
-    horner_init_kernel<<<blocks, 256, 0, st>>>(n, A, bscale / m, P);
+    horner_init_kernel<<<blocks, 256, 0, st>>>(n, ld, Ap, bscale / m, P);
     if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
   }
   double* cur = P;
   double* nxt = Q;
   for (int k = m - 1; k >= 1; --k) {
-    if (square_gemm(n, A, cur, bscale / k, 1.0, nxt, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    if (square_gemm(n, ld, Ap, cur, bscale / k, 1.0, nxt, st) != cudaSuccess) return AFQ_ERR_CUDA;
     double* t = cur;
     cur = nxt;
     nxt = t;
   }
   // squaring
   for (int i = 0; i < s; ++i) {
-    double* dst = (i == s - 1) ? out : nxt;
-    if (square_gemm(n, cur, cur, 1.0, 0.0, dst, st) != cudaSuccess) return AFQ_ERR_CUDA;
-    if (i == s - 1) cur = out;
-    else {
-      double* t = cur;
-      cur = nxt;
-      nxt = t;
-    }
+    if (square_gemm(n, ld, cur, cur, 1.0, 0.0, nxt, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    double* t = cur;
+    cur = nxt;
+    nxt = t;
   }
-  if (s == 0 && cudaMemcpyAsync(out, cur, nn * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-    return AFQ_ERR_CUDA;
+  if (copy2d(n, n, cur, ld, out, n, st) != cudaSuccess) return AFQ_ERR_CUDA;
   return AFQ_OK;
 }
 
@@ -532,21 +602,27 @@ int afq_propagation_intermediates(int32_t norb, int32_t nchol, int32_t walker_ty
   size_t need = 0;
   afq_intermediates_workspace_size(norb, nchol, &need);
   if (work_bytes < need) return AFQ_ERR_WORKSPACE;
-  if (!al16(work) || !al16(rdm1) || !al16(chol)) return AFQ_ERR_ALIGN;
+  if (!al16(work) || !al16(chol)) return AFQ_ERR_ALIGN;
   cudaStream_t st = as_stream(stream);
   const int n = norb, G = nchol;
-  const long long nn = (long long)n * n;
+  const long long nn = (long long)n * n, ld = even(n);
   const int np = walker_type == AFQ_UNRESTRICTED ? 2 : 1;
   int bsum = 0;
   const int nz = vsplits(n, G, &bsum);
   double* v0p = static_cast<double*>(work);
   double* v1p = v0p + even(nz * nn);
   double* hm = v1p + even((long long)kV1Split * nn);
-  double* ew = hm + even(2 * nn);  // expm workspace: 3 nn + 2
+  double* ew = hm + even(2 * nn);  // the exponential's scratch
+  double* cholp = ew + expm_work(n);
+  const double* Bc = chol;
+  if (n & 1) {
+    if (copy2d((long long)G * n, n, chol, n, cholp, ld, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    Bc = cholp;
+  }
   const int blocks = (int)((nn + 255) / 256);
   {
     ProfScope ps(K_MISC, st);
-    // rdm1 is (2, n, n): rho = rdm1[0] + rdm1[1], formed in the expm scratch
+    // rdm1 is (2, n, n): rho = rdm1[0] + rdm1[1], formed in the exponential's scratch
     hmod_kernel<<<blocks, 256, 0, st>>>(nn, 1, rdm1, 1, nullptr, 0, nullptr, 0, 2.0, ew);
     mf_kernel<<<G, 256, 0, st>>>(nn, chol, ew, mf_shifts);
     h0prop_kernel<<<1, 256, 0, st>>>(G, mf_shifts, h0, h0_prop);
@@ -558,8 +634,8 @@ int afq_propagation_intermediates(int32_t norb, int32_t nchol, int32_t walker_ty
   // v0 partials: part[z] = sum_{g in z} L_g L_g
   {
     DgemmArgs a{};
-    a.A = F64Operand{chol, n, nn, 0, kUnsegS};
-    a.B = F64Operand{chol, n, nn, 0, kUnsegS};
+    a.A = F64Operand{Bc, ld, (long long)n * ld, 0, kUnsegS};
+    a.B = F64Operand{Bc, ld, (long long)n * ld, 0, kUnsegS};
     a.M = a.N = a.K = n;
     a.nbatch = G;
     a.bsum = bsum;
@@ -577,7 +653,7 @@ int afq_propagation_intermediates(int32_t norb, int32_t nchol, int32_t walker_ty
   }
   for (int s = 0; s < np; ++s) {
     const int rc = afq_expm(n, hm + s * nn, -0.5 * dt, exp_h1 + s * nn, ew,
-                            (size_t)(3 * even(nn) + 2) * sizeof(double), stream);
+                            (size_t)expm_work(n) * sizeof(double), stream);
     if (rc != AFQ_OK) return rc;
   }
   return AFQ_OK;
@@ -591,18 +667,17 @@ int afq_eigh_desc(int32_t n, const double* A, double* evals, double* evecs, void
   if (work_bytes < (size_t)(2 * even(nn) + 8) * sizeof(double)) return AFQ_ERR_WORKSPACE;
   if (!al16(work)) return AFQ_ERR_ALIGN;
   cudaStream_t st = as_stream(stream);
-  double* Ac = static_cast<double*>(work);
-  double* V = Ac + even(nn);
+  double* Ag = static_cast<double*>(work);
+  double* V = Ag + even(nn);
   int* sweeps = reinterpret_cast<int*>(V + even(nn));
-  if (cudaMemcpyAsync(Ac, A, nn * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-    return AFQ_ERR_CUDA;
   const int npair = ((n + 1) & ~1) / 2;
-  const size_t smem = (size_t)npair * (2 * sizeof(double) + 2 * sizeof(int));
+  size_t smem = (size_t)npair * (2 * sizeof(double) + 2 * sizeof(int)) + 8;
+  if (n <= kJacobiSmemN) smem += (size_t)nn * sizeof(double);
   if (cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return AFQ_ERR_CUDA;
   ProfScope ps(K_MISC, st);
-  jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(n, Ac, V, evals, evecs, sweeps);
+  jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(n, A, Ag, V, evals, evecs, sweeps);
   return cudaGetLastError() == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
 }
 

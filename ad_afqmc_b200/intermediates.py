@@ -74,7 +74,7 @@ def expm(a: torch.Tensor, scale: float = 1.0) -> torch.Tensor:
     a = to_dev(a).contiguous()
     n = int(a.shape[0])
     out = torch.empty_like(a)
-    work = torch.empty(2 * n * n + 8, dtype=torch.float64, device=a.device)
+    work = workspace(n, 1, a.device)  # covers the exponential's scratch
     _lib.check(_lib.lib().afq_expm(n, a.data_ptr(), float(scale), out.data_ptr(), work.data_ptr(),
                                    work.numel() * 8, _lib.stream_handle()), "afq_expm")
     return out
@@ -86,7 +86,7 @@ def eigh_desc(a: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
     n = int(a.shape[0])
     vals = torch.empty(n, dtype=torch.float64, device=a.device)
     vecs = torch.empty(n, n, dtype=torch.float64, device=a.device)
-    work = torch.empty(2 * n * n + 8, dtype=torch.float64, device=a.device)
+    work = torch.empty(2 * n * n + 16, dtype=torch.float64, device=a.device)
     _lib.check(_lib.lib().afq_eigh_desc(n, a.data_ptr(), vals.data_ptr(), vecs.data_ptr(), work.data_ptr(),
                                         work.numel() * 8, _lib.stream_handle()), "afq_eigh_desc")
     return vals, vecs

@@ -361,7 +361,8 @@ int afq_propagation_intermediates(int32_t norb, int32_t nchol, int32_t walker_ty
  * A): scaling and squaring of a truncated Taylor series whose degree follows
  * from the remainder bound for ||scale A / 2^s||_1 <= 1/2.  Synchronizes
  * `stream` once.  Replaces jax.scipy.linalg.expm in propagation.py:422-438.
- * work: at least 2 n^2 + 2 doubles (afq_intermediates_workspace_size covers it). */
+ * work: 3 n m + 8 doubles with m = n rounded up to even
+ * (afq_intermediates_workspace_size(n, 1) bytes cover it). */
 int afq_expm(int32_t n, const double* A, double scale, double* out, void* work, size_t work_bytes,
              void* stream);
 
@@ -371,7 +372,8 @@ int afq_expm(int32_t n, const double* A, double scale, double* out, void* work, 
  * wave_function.get_init_walkers (wavefunctions.py:427-466) are the first
  * nocc columns for rdm1[0] + rdm1[1] (restricted walkers) or rdm1[s]
  * (unrestricted).  Within a degenerate eigenspace the basis may differ from
- * LAPACK's (as it may between LAPACK builds).  work: 2 n^2 + 8 doubles. */
+ * LAPACK's (as it may between LAPACK builds).  work: 2 m + 8 doubles with m =
+ * n^2 rounded up to even.  Up to n = 160 the matrix is rotated in shared memory. */
 int afq_eigh_desc(int32_t n, const double* A, double* evals, double* evecs, void* work,
                   size_t work_bytes, void* stream);
 

@@ -109,21 +109,21 @@ def test_run_afqmc_driver_options(calc_dir, precision):
 def test_run_afqmc_tight_statistics(calc_dir):
     """The energy of the reference's driver test at its own settings (50
     walkers, 10 blocks of 10 x 50 steps, UHF trial, seed 98 in the reference)
-    averaged over 24 independent seeds, so that its standard error drops below
+    averaged over 80 independent seeds, so that its standard error drops below
     0.3 mHa, compared at three combined standard errors with both energies the
     reference asserts (tests/test_driver.py:74-86, one rank, and :19-33, two
     ranks of 50 walkers).  Each reference value is a single run of its own
     random stream: its statistical error is the spread of single runs, which
-    the 24 seeds measure directly (over sqrt(2) for the two-rank run, which
+    the 80 seeds measure directly (over sqrt(2) for the two-rank run, which
     has twice the walkers).  The walker count stays the reference's because
     the population-control bias depends on it."""
     d, e_uhf, meta = calc_dir
     base = dict(meta["driver_options"], precision="fp64")
-    runs = np.array([launch_script.run_afqmc(dict(base, seed=1000 + k), tmpdir=d)[0] for k in range(24)])
+    runs = np.array([launch_script.run_afqmc(dict(base, seed=1000 + k), tmpdir=d)[0] for k in range(80)])
     e_mean = float(runs.mean())
     s_single = float(runs.std(ddof=1))
     s_mean = s_single / np.sqrt(len(runs))
-    print(f"24 runs at the reference settings: E = {e_mean:.6f} +- {s_mean:.6f} Ha "
+    print(f"80 runs at the reference settings: E = {e_mean:.6f} +- {s_mean:.6f} Ha "
           f"(single-run spread {s_single:.6f})")
     assert s_mean < 3e-4
     refs = [(meta["reference_values"]["afqmc_energy_1proc"][0], s_single),
