@@ -11,6 +11,9 @@ per-block scalars, as in stat_utils.py.
 
 from __future__ import annotations
 
+import json
+import pickle
+import time
 import warnings
 from typing import Optional, Tuple
 
@@ -34,6 +37,42 @@ def _run_equilibration(ham, ham_data, prop, prop_data, trial, wave_data, sampler
     return prop_data
 
 
+def _host_prop_data(prop_data: dict) -> dict:
+    """A host copy of prop_data (walkers, weights, overlaps, scalars as NumPy,
+    the counter-based key as (seed, counter)) for pickling."""
+    out = {}
+    for k, v in prop_data.items():
+        if k.startswith("_"):
+            continue
+        if k == "walkers":
+            d = v.data
+            out[k] = [t.cpu().numpy() for t in d] if isinstance(d, list) else d.cpu().numpy()
+        elif isinstance(v, torch.Tensor):
+            out[k] = v.detach().cpu().numpy()
+        elif k == "key":
+            out[k] = (v.seed, v.counter)
+        else:
+            out[k] = v
+    return out
+
+
+def save_walkers(prop_data: dict, n: int, tmpdir: str, rank: int = 0) -> None:
+    """driver._save_walkers (driver.py:985-992): the walker state after block
+    n pickled to ``tmpdir/prop_data_<rank>.bin`` (appended after block 0),
+    copied from the device once per block."""
+    mode = "ab" if n > 0 else "wb"
+    with open(f"{tmpdir}/prop_data_{rank}.bin", mode) as f:
+        pickle.dump(_host_prop_data(prop_data), f)
+
+
+def write_metrics(path: str, energies: np.ndarray, weights: np.ndarray, seconds: float, **extra) -> None:
+    """One JSON line per block (energy, weight) and a closing summary line."""
+    with open(path, "w") as f:
+        for n, (e, w) in enumerate(zip(energies, weights)):
+            f.write(json.dumps({"block": n, "energy": float(e), "weight": float(w)}) + "\n")
+        f.write(json.dumps({"blocks": int(len(energies)), "seconds": float(seconds), **extra}) + "\n")
+
+
 def _warn_nonfinite(e: np.ndarray, w: np.ndarray) -> None:
     """Block energies or weights that are not finite (a population whose
     weights all went to zero gives 0/0) pass through the analysis as in the
@@ -46,8 +85,9 @@ def _warn_nonfinite(e: np.ndarray, w: np.ndarray) -> None:
 
 
 def afqmc_blocks(ham, ham_data, prop, prop_data, trial, wave_data, smp, n_blocks,
-                 field_source=None):
-    """Sampling loop of driver.py:133-168 on one rank; returns (energies, weights, prop_data)."""
+                 field_source=None, save: bool = False, tmpdir: str = "."):
+    """Sampling loop of driver.py:133-168 on one rank; returns (energies, weights, prop_data).
+    ``save``: the reference's ``save_walkers`` option (driver.py:160-161)."""
     energies = torch.zeros(n_blocks, dtype=torch.float64, device=prop_data["weights"].device)
     weights = torch.zeros_like(energies)
     for n in range(n_blocks):
@@ -55,6 +95,8 @@ def afqmc_blocks(ham, ham_data, prop, prop_data, trial, wave_data, smp, n_blocks
         energies[n] = e
         weights[n] = torch.sum(prop_data["weights"])
         prop_data["walkers"] = prop_data["walkers"].orthonormalize()
+        if save:
+            save_walkers(prop_data, n, tmpdir)
         zeta = field_source.uniform() if field_source is not None else prop_data["key"].uniform()
         prop_data["walkers"], prop_data["weights"] = prop_data["walkers"].stochastic_reconfiguration_global(
             prop_data["weights"], zeta)
@@ -77,12 +119,17 @@ def afqmc_energy(ham_data: dict, ham, propagator, trial, wave_data: dict, sample
                              n_sr_blocks=options.get("n_sr_blocks_eql", 5),
                              n_blocks=options.get("n_eql", 1))
     prop_data = _run_equilibration(ham, ham_data, propagator, prop_data, trial, wave_data, sampler_eq)
+    t0 = time.perf_counter()
     energies, weights, prop_data = afqmc_blocks(ham, ham_data, propagator, prop_data, trial, wave_data,
-                                                sampler, sampler.n_blocks)
+                                                sampler, sampler.n_blocks,
+                                                save=bool(options.get("save_walkers", False)), tmpdir=tmpdir)
     e = energies.cpu().numpy()
     w = weights.cpu().numpy()
     _warn_nonfinite(e, w)
     np.savetxt(tmpdir + "/samples_raw.dat", np.stack((w, e)).T)
+    if options.get("metrics_file"):
+        write_metrics(options["metrics_file"], e, w, time.perf_counter() - t0,
+                      walkers=int(propagator.n_walkers), steps_per_block=int(sampler.n_prop_steps))
     clean, _ = stat_utils.reject_outliers(np.stack((w, e)).T, 1)
     return stat_utils.blocking_analysis(clean[:, 0], clean[:, 1], neql=0)
 
@@ -119,6 +166,8 @@ def afqmc_LNOenergy(ham_data: dict, ham, propagator, trial, wave_data: dict, sam
         weights.append(float(torch.sum(prop_data["weights"])))
         orbes.append(float(o))
         prop_data["walkers"] = prop_data["walkers"].orthonormalize()
+        if options.get("save_walkers", False):
+            save_walkers(prop_data, n, tmpdir)
         zeta = prop_data["key"].uniform()
         prop_data["walkers"], prop_data["weights"] = prop_data["walkers"].stochastic_reconfiguration_global(
             prop_data["weights"], zeta)

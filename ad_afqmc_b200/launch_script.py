@@ -76,6 +76,8 @@ def read_options(options: Optional[Dict] = None, tmp_dir: Optional[str] = None) 
     if options["precision"] not in ("fp64", "mixed"):
         raise ValueError(f"precision={options['precision']!r}")
     options["prjlo"] = options.get("prjlo", None)
+    options["save_walkers"] = options.get("save_walkers", False)
+    options["metrics_file"] = options.get("metrics_file", None)
     options["maxError"] = options.get("maxError", 1e-3)
     return options
 

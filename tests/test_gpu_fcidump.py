@@ -130,3 +130,35 @@ def test_run_afqmc_tight_statistics(calc_dir):
             (meta["reference_values"]["afqmc_energy_2proc"][0], s_single / np.sqrt(2.0))]
     for e_ref, s_ref in refs:
         assert abs(e_mean - e_ref) < 3.0 * np.hypot(s_mean, s_ref), (e_mean, s_mean, e_ref, s_ref)
+
+
+def test_save_walkers_and_metrics(calc_dir, tmp_path):
+    """The reference's save_walkers option (driver.py:160-161, 985-992): one
+    pickled host copy of the walker state per block, appended; and the JSON
+    lines of per-block energies and weights."""
+    import json
+    import pickle
+
+    d, _, meta = calc_dir
+    metrics = str(tmp_path / "metrics.jsonl")
+    options = dict(meta["driver_options"], precision="fp64", n_blocks=4, n_walkers=16,
+                   save_walkers=True, metrics_file=metrics)
+    launch_script.run_afqmc(options, tmpdir=d)
+    states = []
+    with open(os.path.join(d, "prop_data_0.bin"), "rb") as f:
+        while True:
+            try:
+                states.append(pickle.load(f))
+            except EOFError:
+                break
+    assert len(states) == 4
+    for st in states:
+        up, dn = st["walkers"]
+        assert up.shape == (16, 6, 3) and dn.shape == (16, 6, 3)
+        # orthonormalized walkers (QR) before the reconfiguration
+        assert np.allclose(np.einsum("wpi,wpj->wij", up.conj(), up), np.eye(3)[None], atol=1e-10)
+        assert st["weights"].shape == (16,)
+    lines = [json.loads(x) for x in open(metrics)]
+    assert [x["block"] for x in lines[:-1]] == [0, 1, 2, 3]
+    assert lines[-1]["blocks"] == 4 and lines[-1]["walkers"] == 16
+    assert all(np.isfinite(x["energy"]) for x in lines[:-1])
