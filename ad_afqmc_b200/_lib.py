@@ -151,6 +151,9 @@ _SIGS = {
                  C.c_int),
     "afq_eigh_desc": ([C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p],
                       C.c_int),
+    "afq_natural_orbitals_workspace_size": ([C.c_int32, C.c_int32, C.POINTER(C.c_size_t)], C.c_int),
+    "afq_natural_orbitals": ([C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.c_size_t, C.c_void_p], C.c_int),
     "afq_check_status": ([C.POINTER(afq_dims), C.c_void_p, C.c_size_t, C.c_void_p], C.c_int),
     "afq_status_flag": ([C.POINTER(afq_dims), C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)], C.c_int),
     "afq_test_wait_timeout": ([C.POINTER(afq_dims), C.c_void_p, C.c_size_t, C.c_uint32, C.c_void_p],

@@ -59,7 +59,8 @@ __global__ void __launch_bounds__(Cfg::NT) fb_gemm_kernel(F64Operand A, F64Opera
 // ---------------------------------------------------------------------------
 // field preparation (one CTA per walker)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void prep_body(int W, int G, long long Gpad, int splitk,
+// one compiled copy for the solo and the grouped kernel (identical rounding)
+__device__ __noinline__ void prep_body(int W, int G, long long Gpad, int splitk,
                                           const double* fbpart, double alpha, const double* fields,
                                           const double* mf, double sdt, double* xt, double* wscal,
                                           double* fb_out, int npc, bf16* xb0, bf16* xb1, bf16* xb2,

@@ -576,7 +576,8 @@ __global__ void __launch_bounds__(kGreenThreads, 4) gj_kernel_grouped(const GjAr
   gj_body(a.W, a.no0, a.no1, a.sbuf, a.sstride, a.bstride, a.wscal, local % a.W, local / a.W);
 }
 
-__device__ __forceinline__ void ovlp_body(int W, int ns, int mult, const double* wscal, double* out,
+// one compiled copy for the solo and the grouped kernel (identical rounding)
+__device__ __noinline__ void ovlp_body(int W, int ns, int mult, const double* wscal, double* out,
                                           int out_stride, int w) {
   if (w >= W) return;
   const double2 d0 = make_double2(wscal[(long long)w * 16 + 4], wscal[(long long)w * 16 + 5]);

@@ -26,9 +26,13 @@
 
 #include <math.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "afqmc_b200.h"
 #include "common.cuh"
 #include "gemm_f64.cuh"
+#include "ops.h"
 #include "profile.cuh"
 
 namespace afq {
@@ -55,7 +59,7 @@ struct DgemmArgs {
   long long ldc, c_bs;
 };
 
-template <class Cfg>
+template <class Cfg, int BMODE = B_KMAJOR>
 __global__ void __launch_bounds__(Cfg::NT) dgemm_kernel(DgemmArgs a) {
   extern __shared__ double smem[];
   const int m0 = blockIdx.x * Cfg::BM, n0 = blockIdx.y * Cfg::BN, z = blockIdx.z;
@@ -67,7 +71,7 @@ __global__ void __launch_bounds__(Cfg::NT) dgemm_kernel(DgemmArgs a) {
     b1 = min(a.nbatch, b0 + a.bsum);
   }
   for (int b = b0; b < b1; ++b)
-    f64_mainloop<Cfg, B_KMAJOR>(acc, a.A, a.B, a.M, a.N, 0, a.K, m0, n0, b, false, smem);
+    f64_mainloop<Cfg, BMODE>(acc, a.A, a.B, a.M, a.N, 0, a.K, m0, n0, b, false, smem);
   double* Cz = a.C + (long long)z * a.c_bs;
   const double* Iz = a.cin ? a.cin + (long long)z * a.cin_bs : nullptr;
   f64_foreach<Cfg>(acc, m0, n0, [&](int m, int n, double v0, double v1) {
@@ -85,15 +89,33 @@ __global__ void __launch_bounds__(Cfg::NT) dgemm_kernel(DgemmArgs a) {
   });
 }
 
-template <class Cfg>
+// B_KMAJOR: B element (k, n) at ptr + k ld + n;  B_NMAJOR: at ptr + n ld + k
+template <class Cfg, int BMODE = B_KMAJOR>
 cudaError_t dgemm(const DgemmArgs& a, int zdim, cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(dgemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)Cfg::SMEM);
+  cudaError_t e = cudaFuncSetAttribute(dgemm_kernel<Cfg, BMODE>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
   if (e != cudaSuccess) return e;
   dim3 grid((a.M + Cfg::BM - 1) / Cfg::BM, (a.N + Cfg::BN - 1) / Cfg::BN, zdim);
   ProfScope ps(K_MISC, st);
-  dgemm_kernel<Cfg><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a);
+  dgemm_kernel<Cfg, BMODE><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a);
   return cudaGetLastError();
+}
+
+// C (M x N, ldc) = alpha A (M x K, lda) B, B k-major (K x N, ldb) or n-major (N x K, ldb)
+template <int BMODE>
+cudaError_t gemm2(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
+                  double alpha, double* C, long long ldc, cudaStream_t st) {
+  DgemmArgs a{};
+  a.A = F64Operand{A, lda, 0, 0, kUnsegS};
+  a.B = F64Operand{B, ldb, 0, 0, kUnsegS};
+  a.M = M;
+  a.N = N;
+  a.K = K;
+  a.nbatch = 1;
+  a.alpha = alpha;
+  a.C = C;
+  a.ldc = ldc;
+  return dgemm<CfgS, BMODE>(a, 1, st);
 }
 
 // plain square product C = alpha A B (+ diag I), n x n row-major, all with the
@@ -166,13 +188,14 @@ __global__ void sym_kernel(int n, double* h1, double* hrot, long long ldh, int u
   }
 }
 
-// out (cols x rows, row stride ldo) = in (rows x cols)^T
-__global__ void transpose_kernel(int rows, int cols, const double* in, double* out, long long ldo) {
+// out (cols x rows, row stride ldo) = in (rows x cols, row stride ldi)^T
+__global__ void transpose_kernel(int rows, int cols, const double* in, long long ldi, double* out,
+                                 long long ldo) {
   const long long nn = (long long)rows * cols;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nn;
        e += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(e / cols), c = (int)(e % cols);
-    out[(long long)c * ldo + r] = in[e];
+    out[(long long)c * ldo + r] = in[(long long)r * ldi + c];
   }
 }
 
@@ -274,7 +297,6 @@ __global__ void horner_init_kernel(int n, long long ld, const double* B, double 
 constexpr int kJacobiThreads = 1024;
 constexpr int kJacobiMaxSweeps = 40;
 constexpr int kJacobiMaxN = 2048;
-constexpr int kJacobiSmemN = 160;  // matrix in shared memory up to this order
 
 // round-robin pairing: position k of round r (n even, positions 0..n-1)
 __device__ __forceinline__ int rr_index(int k, int r, int n) {
@@ -282,41 +304,67 @@ __device__ __forceinline__ int rr_index(int k, int r, int n) {
   return 1 + (k - 1 + r) % (n - 1);
 }
 
-// A (n x n, row stride lda, symmetric; shared or global memory) is
-// overwritten; V (global, n x n) receives the eigenvectors as columns;
-// evals/evecs: sorted descending.  One round applies the npair disjoint
-// rotations of the round-robin ordering at once: the 2x2 block of A on rows
-// {p1, q1} and columns {p2, q2} becomes J1^T A J2 (J = [[c, s], [-s, c]] on
-// (p, q)), and the rotated pair's own off-diagonal element is set to zero.
-// The padding index n (odd n) is a phantom without rotations.  Sweeps stop
-// when the off-diagonal Frobenius norm is at most 4 n eps of the matrix's.
-__device__ void jacobi_body(int n, double* A, long long lda, double* V, double* evals, double* evecs,
+// Symmetric matrix storage: the packed upper triangle in shared memory
+// (PACKED) or the full matrix in global memory.
+template <bool PACKED>
+struct SymMat {
+  double* a;
+  int n;
+  __device__ __forceinline__ double* at(int i, int j) const {
+    if (PACKED) {
+      if (i > j) {
+        const int t = i;
+        i = j;
+        j = t;
+      }
+      return a + (i * (2 * n - i + 1)) / 2 + (j - i);
+    }
+    return a + (long long)i * n + j;
+  }
+};
+__host__ __device__ inline long long packed_len(int n) { return (long long)n * (n + 1) / 2; }
+
+// Eigenpairs of the symmetric matrix in M: one round applies the npair
+// disjoint rotations of the round-robin ordering at once.  The 2x2 block of A
+// on rows {p1, q1} and columns {p2, q2} becomes J1^T A J2 (J = [[c, s], [-s,
+// c]] on (p, q)); only blocks with k1 <= k2 are updated (the others are their
+// transposes, the same storage), and the rotated pair's off-diagonal element
+// is set to zero.  The eigenvectors accumulate transposed in VT (global, row p
+// of VT is column p of V, so a rotation updates two contiguous rows).  The
+// padding index n (odd n) is a phantom without rotations.  Sweeps stop when
+// the off-diagonal Frobenius norm is at most 4 n eps of the matrix's, or when a
+// sweep no longer reduces it (the rounding floor).
+template <bool PACKED>
+__device__ void jacobi_body(const SymMat<PACKED> M, double* VT, double* evals, double* evecs,
                             int* sweeps_out, double* cs, double* sn, int* pp, int* qq) {
   __shared__ double red[32];
+  const int n = M.n;
   const int np = (n + 1) & ~1;
   const int npair = np / 2;
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int e = tid; e < n * n; e += nt) V[e] = ((e / n) == (e % n)) ? 1.0 : 0.0;
+  for (int e = tid; e < n * n; e += nt) VT[e] = ((e / n) == (e % n)) ? 1.0 : 0.0;
   double fro = 0.0;
   for (int e = tid; e < n * n; e += nt) {
-    const double x = A[(long long)(e / n) * lda + e % n];
+    const double x = *M.at(e / n, e % n);
     fro += x * x;
   }
   fro = block_sum(fro, red);
   const double eps = 2.220446049250313e-16;
   const double tol2 = fro * (4.0 * n * eps) * (4.0 * n * eps);
+  double prev = -1.0;
   int sweep = 0;
   for (; sweep < kJacobiMaxSweeps; ++sweep) {
     double off = 0.0;
     for (int e = tid; e < n * n; e += nt) {
       const int i = e / n, j = e - i * n;
       if (i != j) {
-        const double x = A[(long long)i * lda + j];
+        const double x = *M.at(i, j);
         off += x * x;
       }
     }
     off = block_sum(off, red);
-    if (off <= tol2 || fro == 0.0) break;
+    if (off <= tol2 || fro == 0.0 || (prev >= 0.0 && off >= prev)) break;
+    prev = off;
     for (int r = 0; r < np - 1; ++r) {
       // rotation parameters (Golub & Van Loan, Algorithm 8.5.1, sym.schur2)
       for (int k = tid; k < npair; k += nt) {
@@ -328,9 +376,9 @@ __device__ void jacobi_body(int n, double* A, long long lda, double* V, double* 
         }
         double c = 1.0, s = 0.0;
         if (q < n) {
-          const double apq = A[(long long)p * lda + q];
+          const double apq = *M.at(p, q);
           if (apq != 0.0) {
-            const double app = A[(long long)p * lda + p], aqq = A[(long long)q * lda + q];
+            const double app = *M.at(p, p), aqq = *M.at(q, q);
             const double tau = (aqq - app) / (2.0 * apq);
             const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
             c = 1.0 / sqrt(1.0 + t * t);
@@ -343,66 +391,88 @@ __device__ void jacobi_body(int n, double* A, long long lda, double* V, double* 
         qq[k] = q < n ? q : -1;
       }
       __syncthreads();
-      // A <- J^T A J, one 2x2 block per (k1, k2)
-      for (int it = tid; it < npair * npair; it += nt) {
-        const int k1 = it / npair, k2 = it - k1 * npair;
+      // A <- J^T A J, one 2x2 block per (k1 <= k2)
+      const int nblk = npair * (npair + 1) / 2;
+      for (int it = tid; it < nblk; it += nt) {
+        // it -> (k1, k2), k1 <= k2, row-major over the upper triangle of pairs
+        int k1 = (int)((2.0 * npair + 1.0 - sqrt((2.0 * npair + 1.0) * (2.0 * npair + 1.0) - 8.0 * it)) * 0.5);
+        while (k1 > 0 && k1 * (2 * npair - k1 + 1) / 2 > it) --k1;
+        while ((k1 + 1) * (2 * npair - k1) / 2 <= it) ++k1;
+        const int k2 = k1 + (it - k1 * (2 * npair - k1 + 1) / 2);
         const int p1 = pp[k1], q1 = qq[k1], p2 = pp[k2], q2 = qq[k2];
         const double c1 = cs[k1], s1 = sn[k1], c2 = cs[k2], s2 = sn[k2];
         if (s1 == 0.0 && s2 == 0.0) continue;
-        double* rp = A + (long long)p1 * lda;
-        double* rq = q1 >= 0 ? A + (long long)q1 * lda : nullptr;
-        const double x00 = rp[p2], x01 = q2 >= 0 ? rp[q2] : 0.0;
-        const double x10 = rq ? rq[p2] : 0.0, x11 = (rq && q2 >= 0) ? rq[q2] : 0.0;
-        // columns: [y0 y1] = [x0 x1] J2
+        if (k1 == k2) {  // the pair's own symmetric 2x2 block
+          if (q1 < 0) continue;
+          const double x00 = *M.at(p1, p1), x01 = *M.at(p1, q1), x11 = *M.at(q1, q1);
+          const double a00 = c1 * x00 - s1 * x01, a01 = s1 * x00 + c1 * x01;
+          const double a10 = c1 * x01 - s1 * x11, a11 = s1 * x01 + c1 * x11;
+          *M.at(p1, p1) = c1 * a00 - s1 * a10;
+          *M.at(q1, q1) = s1 * a01 + c1 * a11;
+          *M.at(p1, q1) = 0.0;
+          if (!PACKED) *M.at(q1, p1) = 0.0;
+          continue;
+        }
+        const double x00 = *M.at(p1, p2);
+        const double x01 = q2 >= 0 ? *M.at(p1, q2) : 0.0;
+        const double x10 = q1 >= 0 ? *M.at(q1, p2) : 0.0;
+        const double x11 = (q1 >= 0 && q2 >= 0) ? *M.at(q1, q2) : 0.0;
+        // columns: [y0 y1] = [x0 x1] J2, then rows: J1^T
         const double a00 = c2 * x00 - s2 * x01, a01 = s2 * x00 + c2 * x01;
         const double a10 = c2 * x10 - s2 * x11, a11 = s2 * x10 + c2 * x11;
-        // rows: J1^T
-        double b00 = c1 * a00 - s1 * a10, b01 = c1 * a01 - s1 * a11;
-        double b10 = s1 * a00 + c1 * a10, b11 = s1 * a01 + c1 * a11;
-        if (k1 == k2 && s1 != 0.0) {
-          b01 = 0.0;
-          b10 = 0.0;
+        const double b00 = c1 * a00 - s1 * a10, b01 = c1 * a01 - s1 * a11;
+        const double b10 = s1 * a00 + c1 * a10, b11 = s1 * a01 + c1 * a11;
+        *M.at(p1, p2) = b00;
+        if (!PACKED) *M.at(p2, p1) = b00;
+        if (q2 >= 0) {
+          *M.at(p1, q2) = b01;
+          if (!PACKED) *M.at(q2, p1) = b01;
         }
-        rp[p2] = b00;
-        if (q2 >= 0) rp[q2] = b01;
-        if (rq) {
-          rq[p2] = b10;
-          if (q2 >= 0) rq[q2] = b11;
+        if (q1 >= 0) {
+          *M.at(q1, p2) = b10;
+          if (!PACKED) *M.at(p2, q1) = b10;
+          if (q2 >= 0) {
+            *M.at(q1, q2) = b11;
+            if (!PACKED) *M.at(q2, q1) = b11;
+          }
         }
       }
-      // V <- V J
+      // V <- V J: rows p, q of VT
       for (int it = tid; it < npair * n; it += nt) {
         const int k = it / n, i = it - k * n;
         const int p = pp[k], q = qq[k];
-        const double c = cs[k], s = sn[k];
+        const double s = sn[k];
         if (q < 0 || s == 0.0) continue;
-        double* vr = V + (long long)i * n;
-        const double u = vr[p], w = vr[q];
-        vr[p] = c * u - s * w;
-        vr[q] = s * u + c * w;
+        const double c = cs[k];
+        double* vp = VT + (long long)p * n + i;
+        double* vq = VT + (long long)q * n + i;
+        const double u = *vp, w = *vq;
+        *vp = c * u - s * w;
+        *vq = s * u + c * w;
       }
       __syncthreads();
     }
   }
   // descending order: rank of eigenvalue i (ties by index)
   for (int i = tid; i < n; i += nt) {
-    const double li = A[(long long)i * lda + i];
+    const double li = *M.at(i, i);
     int rank = 0;
     for (int j = 0; j < n; ++j) {
-      const double lj = A[(long long)j * lda + j];
+      const double lj = *M.at(j, j);
       if (lj > li || (lj == li && j < i)) ++rank;
     }
     evals[rank] = li;
-    for (int row = 0; row < n; ++row) evecs[(long long)row * n + rank] = V[(long long)row * n + i];
+    for (int row = 0; row < n; ++row) evecs[(long long)row * n + rank] = VT[(long long)i * n + row];
   }
   if (tid == 0 && sweeps_out) *sweeps_out = sweep;
 }
 
 // A: the input matrix (n x n, ld n, global, read only); Ag: global scratch
-// (n x n) used when the matrix does not fit shared memory
-__global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(int n, const double* A, double* Ag,
-                                                                double* V, double* evals,
-                                                                double* evecs, int* sweeps_out) {
+// (n x n) for the matrix when its packed upper triangle does not fit shared memory
+__global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(int n, int packed, const double* A,
+                                                                double* Ag, double* VT,
+                                                                double* evals, double* evecs,
+                                                                int* sweeps_out) {
   extern __shared__ double js[];
   const int npair = ((n + 1) & ~1) / 2;
   double* cs = js;
@@ -410,11 +480,97 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_kernel(int n, const dou
   int* pp = reinterpret_cast<int*>(sn + npair);
   int* qq = pp + npair;
   double* As = reinterpret_cast<double*>(qq + npair);  // 24 npair bytes in: 8-byte aligned
-  const bool in_smem = n <= kJacobiSmemN;
-  double* M = in_smem ? As : Ag;
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) M[e] = A[e];
+  if (packed) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int i = e / n, j = e - i * n;
+      if (i <= j) As[(i * (2 * n - i + 1)) / 2 + (j - i)] = A[e];
+    }
+    __syncthreads();
+    jacobi_body<true>(SymMat<true>{As, n}, VT, evals, evecs, sweeps_out, cs, sn, pp, qq);
+  } else {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) Ag[e] = A[e];
+    __syncthreads();
+    jacobi_body<false>(SymMat<false>{Ag, n}, VT, evals, evecs, sweeps_out, cs, sn, pp, qq);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// natural orbitals by subspace iteration
+// ---------------------------------------------------------------------------
+// In place on the p x p Gram matrix S (row stride ld): S = R^T R (Cholesky,
+// R upper triangular), then S <- R^-T (lower triangular; the strict upper
+// part zeroed).  One CTA; p <= kNatMaxP.  Returns status in *ok (0: not
+// positive definite).
+constexpr int kNatMaxP = 72;  // subspace width: up to 64 orbitals plus 8
+__global__ void __launch_bounds__(256) chol_inv_kernel(int p, double* S, long long ld, int* ok) {
+  __shared__ double R[kNatMaxP * (kNatMaxP + 1)];
+  __shared__ int bad;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int lr = p + 1;
+  for (int e = tid; e < p * p; e += nt) R[(e / p) * lr + e % p] = S[(long long)(e / p) * ld + e % p];
+  if (tid == 0) bad = 0;
   __syncthreads();
-  jacobi_body(n, M, n, V, evals, evecs, sweeps_out, cs, sn, pp, qq);
+  // right-looking Cholesky, upper factor in R (rows k: R[k][k..p))
+  for (int k = 0; k < p; ++k) {
+    if (tid == 0) {
+      const double d = R[k * lr + k];
+      if (!(d > 0.0)) bad = 1;
+      R[k * lr + k] = d > 0.0 ? sqrt(d) : 1.0;
+    }
+    __syncthreads();
+    const double rkk = R[k * lr + k];
+    for (int j = k + 1 + tid; j < p; j += nt) R[k * lr + j] /= rkk;
+    __syncthreads();
+    for (int e = tid; e < (p - k - 1) * (p - k - 1); e += nt) {
+      const int i = k + 1 + e / (p - k - 1), j = k + 1 + e % (p - k - 1);
+      if (j >= i) R[i * lr + j] -= R[k * lr + i] * R[k * lr + j];
+    }
+    __syncthreads();
+  }
+  // R^-1 by back substitution, column by column (thread per column)
+  for (int c = tid; c < p; c += nt) {
+    // solve R x = e_c, x stored in column c of S's upper part (x_i = 0 for i > c)
+    for (int i = p - 1; i >= 0; --i) {
+      double v = (i == c) ? 1.0 : 0.0;
+      if (i <= c)
+        for (int j = i + 1; j <= c; ++j) v -= R[i * lr + j] * S[(long long)j * ld + c];
+      S[(long long)i * ld + c] = i <= c ? v / R[i * lr + i] : 0.0;
+    }
+  }
+  __syncthreads();
+  // transpose in place: S <- (R^-1)^T (lower)
+  for (int e = tid; e < p * p; e += nt) {
+    const int i = e / p, j = e % p;
+    if (i < j) {
+      const double a = S[(long long)i * ld + j];
+      S[(long long)j * ld + i] = a;
+      S[(long long)i * ld + j] = 0.0;
+    }
+  }
+  if (tid == 0) *ok = bad ? 0 : 1;
+}
+
+// residual of the Ritz pairs: res[c] = || (Z^T rho)[c] - theta_c Z^T[c] ||  for c < k
+// (ZR = Z^T rho, ZT = Z^T, rows of length n, stride ld); one warp per row
+__global__ void ritz_residual_kernel(int k, int n, long long ld, const double* ZR, const double* ZT,
+                                     const double* theta, double* res) {
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (c >= k) return;
+  double s = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    const double r = ZR[(long long)c * ld + i] - theta[c] * ZT[(long long)c * ld + i];
+    s += r * r;
+  }
+  s = warp_sum(s);
+  if (lane == 0) res[c] = sqrt(s);
+}
+
+size_t jacobi_smem(int n, bool* packed) {
+  const int npair = ((n + 1) & ~1) / 2;
+  const size_t base = (size_t)npair * (2 * sizeof(double) + 2 * sizeof(int)) + 8;
+  const size_t full = base + (size_t)packed_len(n) * sizeof(double);
+  *packed = full <= 220 * 1024;
+  return *packed ? full : base;
 }
 
 int vsplits(int n, int G, int* bsum) {
@@ -496,7 +652,7 @@ int afq_measurement_intermediates(int32_t norb, const int32_t nocc[2], int32_t n
     double* mt = mot + s * hs;
     {
       ProfScope ps(K_MISC, st);
-      transpose_kernel<<<(int)(((long long)n * no + 255) / 256), 256, 0, st>>>(n, no, mo[s], mt, ld);
+      transpose_kernel<<<(int)(((long long)n * no + 255) / 256), 256, 0, st>>>(n, no, mo[s], no, mt, ld);
       if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
     }
     // rot_h1[s] = mo^T h (no x n)
@@ -659,6 +815,137 @@ int afq_propagation_intermediates(int32_t norb, int32_t nchol, int32_t walker_ty
   return AFQ_OK;
 }
 
+int afq_natural_orbitals_workspace_size(int32_t n, int32_t k, size_t* bytes) {
+  if (!bytes) return AFQ_ERR_NULL;
+  if (n <= 0 || k <= 0 || k > n || n > kJacobiMaxN || k + 8 > kNatMaxP) return AFQ_ERR_SHAPE;
+  const long long ld = even(n);
+  const int p = std::min(n, k + 8);
+  const long long pp = even(p);
+  // X^T, Y^T, Z^T (p x ld), small p x pp matrices (Gram / H, U, scratch for the
+  // Ritz values and residuals), then either the padded rdm (odd n) or the
+  // full-eigensolver fallback (values, vectors and its scratch)
+  const long long nn2 = even((long long)n * n);
+  long long d = 3 * p * ld + 4 * p * pp + 4 * pp + std::max((long long)n * ld, ld + nn2 + 2 * nn2 + 8) + 64;
+  *bytes = (size_t)d * sizeof(double);
+  return AFQ_OK;
+}
+
+int afq_natural_orbitals(int32_t n, int32_t k, const double* rdm, double* orbs, double* occ, void* work,
+                         size_t work_bytes, void* stream) {
+  if (!rdm || !orbs || !work) return AFQ_ERR_NULL;
+  size_t need = 0;
+  int rc = afq_natural_orbitals_workspace_size(n, k, &need);
+  if (rc != AFQ_OK) return rc;
+  if (work_bytes < need) return AFQ_ERR_WORKSPACE;
+  if (!al16(work) || !al16(rdm)) return AFQ_ERR_ALIGN;
+  cudaStream_t st = as_stream(stream);
+  const long long ld = even(n);
+  const int p = std::min(n, k + 8);
+  const long long pp = even(p);
+  double* XT = static_cast<double*>(work);  // p x ld
+  double* YT = XT + p * ld;
+  double* ZT = YT + p * ld;
+  double* S = ZT + p * ld;   // p x pp
+  double* U = S + p * pp;    // p x pp (eigenvectors of H as columns)
+  double* H = U + p * pp;    // p x pp
+  double* T2 = H + p * pp;   // p x pp
+  double* theta = T2 + p * pp;
+  double* res = theta + pp;
+  int* ok = reinterpret_cast<int*>(res + pp);
+  double* full = reinterpret_cast<double*>(ok) + 2 * pp;  // fallback scratch
+  double* rho = full;        // rdm with padded rows when n is odd (inside the fallback space)
+  const double* R = rdm;
+  if (n & 1) {
+    if (copy2d(n, n, rdm, n, rho, ld, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    R = rho;
+  }
+  // start: p deterministic Gaussian rows
+  if (launch_normal(XT, (long long)p * ld, 0x5eedULL, 0, st) != cudaSuccess) return AFQ_ERR_CUDA;
+  const int max_iter = 40;
+  std::vector<double> hres(k), hth(p);
+  int hok = 0;
+  for (int it = 0; it < max_iter; ++it) {
+    // Y^T = X^T rho ; orthonormalize: S = Y^T Y, S = R^-T, X^T = R^-T Y^T (twice: CholeskyQR2)
+    if (gemm2<B_KMAJOR>(p, n, n, XT, ld, R, ld, 1.0, YT, ld, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    for (int pass = 0; pass < 2; ++pass) {
+      double* src = pass == 0 ? YT : XT;
+      double* dst = pass == 0 ? XT : YT;
+      if (gemm2<B_NMAJOR>(p, p, n, src, ld, src, ld, 1.0, S, pp, st) != cudaSuccess) return AFQ_ERR_CUDA;
+      chol_inv_kernel<<<1, 256, 0, st>>>(p, S, pp, ok);
+      if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+      if (gemm2<B_KMAJOR>(p, n, p, S, pp, src, ld, 1.0, dst, ld, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    }
+    // Q^T in YT.  Rayleigh-Ritz: T^T = Q^T rho (in XT), H = Q^T T (p x p)
+    if (gemm2<B_KMAJOR>(p, n, n, YT, ld, R, ld, 1.0, XT, ld, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    if (gemm2<B_NMAJOR>(p, p, n, YT, ld, XT, ld, 1.0, H, pp, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    if (pp != p) {  // the small eigensolver reads a dense p x p matrix
+      if (copy2d(p, p, H, pp, T2, p, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    } else if (cudaMemcpyAsync(T2, H, sizeof(double) * p * p, cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+      return AFQ_ERR_CUDA;
+    }
+    bool packed = false;
+    const size_t smem = jacobi_smem(p, &packed);
+    if (!packed) return AFQ_ERR_SHAPE;
+    if (cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return AFQ_ERR_CUDA;
+    {
+      ProfScope ps(K_MISC, st);
+      // eigenvalues (descending) into theta, eigenvectors as columns of U (p x p, dense)
+      jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(p, 1, T2, nullptr, H, theta, U, nullptr);
+      if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+    }
+    // Ritz vectors Z^T = U^T Q^T: U^T as the A operand (p x p): transpose U into S
+    {
+      ProfScope ps(K_MISC, st);
+      transpose_kernel<<<(p * p + 255) / 256, 256, 0, st>>>(p, p, U, p, S, pp);
+      if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+    }
+    if (gemm2<B_KMAJOR>(p, n, p, S, pp, YT, ld, 1.0, ZT, ld, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    // residuals of the first k: (Z^T rho) in XT
+    if (gemm2<B_KMAJOR>(k, n, n, ZT, ld, R, ld, 1.0, XT, ld, st) != cudaSuccess) return AFQ_ERR_CUDA;
+    {
+      ProfScope ps(K_MISC, st);
+      ritz_residual_kernel<<<(k + 7) / 8, 256, 0, st>>>(k, n, ld, XT, ZT, theta, res);
+      if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+    }
+    if (cudaMemcpyAsync(hres.data(), res, sizeof(double) * k, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(hth.data(), theta, sizeof(double) * p, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(&hok, ok, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return AFQ_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return AFQ_ERR_CUDA;
+    if (!hok) break;  // rank-deficient iterate: use the full eigensolver
+    double scale = 0.0, worst = 0.0;
+    for (int i = 0; i < p; ++i) scale = std::max(scale, fabs(hth[i]));
+    for (int i = 0; i < k; ++i) worst = std::max(worst, hres[i]);
+    if (worst <= 1e-13 * std::max(scale, 1e-300) * sqrt((double)n)) {
+      // converged: orbitals = (Z^T)^T restricted to k columns, occupations theta[0..k)
+      {
+        ProfScope ps(K_MISC, st);
+        transpose_kernel<<<(int)(((long long)k * n + 255) / 256), 256, 0, st>>>(k, n, ZT, ld, orbs, k);
+        if (cudaGetLastError() != cudaSuccess) return AFQ_ERR_CUDA;
+      }
+      if (occ && cudaMemcpyAsync(occ, theta, sizeof(double) * k, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return AFQ_ERR_CUDA;
+      return AFQ_OK;
+    }
+    // next iterate: X^T = Z^T (all p Ritz vectors)
+    if (cudaMemcpyAsync(XT, ZT, sizeof(double) * p * ld, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return AFQ_ERR_CUDA;
+  }
+  // not converged (nearly equal occupations at the cut): the full eigensolver
+  double* vals = full;  // n
+  double* vecs = vals + ld;  // n x n
+  double* jw = vecs + even((long long)n * n);  // its own scratch (16-byte aligned)
+  rc = afq_eigh_desc(n, rdm, vals, vecs, jw, (size_t)(2 * even((long long)n * n) + 8) * sizeof(double),
+                     stream);
+  if (rc != AFQ_OK) return rc;
+  if (copy2d(n, k, vecs, n, orbs, k, st) != cudaSuccess) return AFQ_ERR_CUDA;
+  if (occ && cudaMemcpyAsync(occ, vals, sizeof(double) * k, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return AFQ_ERR_CUDA;
+  return AFQ_OK;
+}
+
 int afq_eigh_desc(int32_t n, const double* A, double* evals, double* evecs, void* work,
                   size_t work_bytes, void* stream) {
   if (!A || !evals || !evecs || !work) return AFQ_ERR_NULL;
@@ -670,14 +957,13 @@ int afq_eigh_desc(int32_t n, const double* A, double* evals, double* evecs, void
   double* Ag = static_cast<double*>(work);
   double* V = Ag + even(nn);
   int* sweeps = reinterpret_cast<int*>(V + even(nn));
-  const int npair = ((n + 1) & ~1) / 2;
-  size_t smem = (size_t)npair * (2 * sizeof(double) + 2 * sizeof(int)) + 8;
-  if (n <= kJacobiSmemN) smem += (size_t)nn * sizeof(double);
+  bool packed = false;
+  const size_t smem = jacobi_smem(n, &packed);
   if (cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return AFQ_ERR_CUDA;
   ProfScope ps(K_MISC, st);
-  jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(n, A, Ag, V, evals, evecs, sweeps);
+  jacobi_kernel<<<1, kJacobiThreads, smem, st>>>(n, packed ? 1 : 0, A, Ag, V, evals, evecs, sweeps);
   return cudaGetLastError() == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
 }
 

@@ -17,7 +17,8 @@ namespace {
 // ---------------------------------------------------------------------------
 constexpr int kWeightThreads = 1024;
 
-__device__ __forceinline__ void weight_body(int W, double dt, const double* scal, const double* wscal,
+// one compiled copy for the solo and the grouped kernel (identical rounding)
+__device__ __noinline__ void weight_body(int W, double dt, const double* scal, const double* wscal,
                                             double* weights, double* overlaps, double* scalars) {
   __shared__ double red[kWeightThreads / 32];
   const double sdt = sqrt(dt);

@@ -80,8 +80,9 @@ def expm(a: torch.Tensor, scale: float = 1.0) -> torch.Tensor:
     return out
 
 
-def eigh_desc(a: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
-    """(eigenvalues descending, eigenvectors as columns in that order)."""
+def eigh_desc(a: torch.Tensor, return_sweeps: bool = False):
+    """(eigenvalues descending, eigenvectors as columns in that order); with
+    ``return_sweeps`` also the number of Jacobi sweeps (synchronizes)."""
     a = to_dev(a).contiguous()
     n = int(a.shape[0])
     vals = torch.empty(n, dtype=torch.float64, device=a.device)
@@ -89,9 +90,25 @@ def eigh_desc(a: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
     work = torch.empty(2 * n * n + 16, dtype=torch.float64, device=a.device)
     _lib.check(_lib.lib().afq_eigh_desc(n, a.data_ptr(), vals.data_ptr(), vecs.data_ptr(), work.data_ptr(),
                                         work.numel() * 8, _lib.stream_handle()), "afq_eigh_desc")
+    if return_sweeps:
+        nn2 = 2 * ((n * n + 1) // 2 * 2)  # the sweep count follows the two (n x n) buffers
+        return vals, vecs, int(work.view(torch.int32)[2 * nn2].item())
     return vals, vecs
 
 
-def natural_orbitals(rdm: torch.Tensor, k: int) -> torch.Tensor:
-    """The k natural orbitals of largest occupation, (N, k) float64."""
-    return eigh_desc(rdm)[1][:, :k].contiguous()
+def natural_orbitals(rdm: torch.Tensor, k: int, return_occ: bool = False):
+    """The k natural orbitals of largest occupation, (N, k) float64
+    (afq_natural_orbitals: subspace iteration with Rayleigh-Ritz, the full
+    Jacobi eigensolver when the occupations at the cut are too close)."""
+    rdm = to_dev(rdm).contiguous()
+    n = int(rdm.shape[0])
+    size = C.c_size_t()
+    _lib.check(_lib.lib().afq_natural_orbitals_workspace_size(n, int(k), C.byref(size)),
+               "afq_natural_orbitals_workspace_size")
+    work = torch.empty((size.value + 7) // 8, dtype=torch.float64, device=rdm.device)
+    orbs = torch.empty(n, int(k), dtype=torch.float64, device=rdm.device)
+    occ = torch.empty(int(k), dtype=torch.float64, device=rdm.device)
+    _lib.check(_lib.lib().afq_natural_orbitals(n, int(k), rdm.data_ptr(), orbs.data_ptr(), occ.data_ptr(),
+                                               work.data_ptr(), work.numel() * 8, _lib.stream_handle()),
+               "afq_natural_orbitals")
+    return (orbs, occ) if return_occ else orbs

@@ -377,6 +377,20 @@ int afq_expm(int32_t n, const double* A, double scale, double* out, void* work, 
 int afq_eigh_desc(int32_t n, const double* A, double* evals, double* evecs, void* work,
                   size_t work_bytes, void* stream);
 
+/* The k natural orbitals of largest occupation of a symmetric density matrix
+ * rdm (n, n) (e.g. rdm1[0] + rdm1[1]): orbs (n, k) row-major, occupations
+ * occ (k,) descending (may be NULL).  This is what wave_function.get_init_walkers
+ * (wavefunctions.py:427-466) takes from eigh.  Subspace iteration on k + 8
+ * vectors (orthonormalized by CholeskyQR2) with a Rayleigh-Ritz step (Jacobi
+ * on the projected matrix) until every Ritz residual is below 1e-13 of the
+ * spectral radius (one iteration for a projector density); when that does not
+ * happen within 40 iterations (occupations too close at the cut) the full
+ * afq_eigh_desc.  Synchronizes `stream` once per iteration.  k <= 64.
+ * work: afq_natural_orbitals_workspace_size() bytes. */
+int afq_natural_orbitals_workspace_size(int32_t n, int32_t k, size_t* bytes);
+int afq_natural_orbitals(int32_t n, int32_t k, const double* rdm, double* orbs, double* occ, void* work,
+                         size_t work_bytes, void* stream);
+
 /* Device-side failure status of a workspace (no counterpart in the reference,
  * whose XLA kernels have no waits of their own; its only guards are the
  * numerical masks of propagation.py:321-331 and the driver's check of the

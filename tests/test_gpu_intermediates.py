@@ -120,3 +120,28 @@ def test_initial_walkers_correlated_density():
     w = _np(trial.get_init_walkers(wave, 2, "restricted").data)[0].real
     ref = np.linalg.eigh(2 * rdm)[1][:, ::-1][:, :no]
     assert np.allclose(np.abs(np.sum(w * ref, axis=0)), 1.0, atol=1e-10)
+
+
+@pytest.mark.parametrize("gap", [0.5, 1e-3])
+def test_natural_orbitals_subspace_and_fallback(gap):
+    """afq_natural_orbitals: a clear gap at the cut converges by subspace
+    iteration; a gap of 1e-3 does not within its iteration limit and takes the
+    full Jacobi eigensolver.  Either way the span of the k orbitals is LAPACK's
+    (its projector to 1e-10) and the occupations match."""
+    from ad_afqmc_b200 import intermediates
+
+    n, k = 73, 17
+    rng = np.random.default_rng(5)
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    occ = np.concatenate([1.0 + 0.9 * rng.random(k), (1.0 - gap) * rng.random(n - k)])
+    occ[k - 1] = 1.0
+    occ[k] = 1.0 - gap
+    rdm = (q * occ) @ q.T
+    orbs, o = intermediates.natural_orbitals(torch.as_tensor(rdm, device="cuda"), k, return_occ=True)
+    orbs, o = _np(orbs), _np(o)
+    ref = np.sort(occ)[::-1][:k]
+    assert np.allclose(o, ref, atol=1e-12)
+    w, v = np.linalg.eigh(rdm)
+    vk = v[:, ::-1][:, :k]
+    assert np.abs(orbs @ orbs.T - vk @ vk.T).max() < 1e-10
+    assert np.allclose(orbs.T @ orbs, np.eye(k), atol=1e-12)
