@@ -421,7 +421,7 @@ cudaError_t launch_weight_grouped(const WeightArgs* args, int n, cudaStream_t st
 cudaError_t launch_qr(const Layout& L, double* const walkers[2], double* norms, double* work,
                       cudaStream_t st) {
   const size_t smem = size_t(L.N) * (L.nomax + 1) * sizeof(double2);
-  const int use_smem = smem <= 200 * 1024;
+  const int use_smem = smem <= 200 * 1024 && L.tune.qr_mode != 2;
   const size_t dyn = use_smem ? smem : 0;
   cudaError_t e =
       cudaFuncSetAttribute(qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);

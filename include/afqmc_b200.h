@@ -292,7 +292,9 @@ typedef struct afq_tuning {
                        /* walkers last read stay in L2 for the next launch), 1 forward     */
   int32_t prop_chunk;  /* propagator K accumulation: 0 chunks of four 64-wide K blocks     */
                        /* summed in FP32 round-to-nearest, 1 the whole K in one chain     */
-  int32_t reserved[6];
+  int32_t qr_mode;     /* QR of the walkers: 0 built-in choice, 1 walker in shared memory   */
+                       /* (when it fits), 2 in place in global memory                       */
+  int32_t reserved[5];
 } afq_tuning;
 
 int afq_set_tuning(const afq_dims* d, const afq_tuning* t);

@@ -182,6 +182,29 @@ def test_qr_matches_lapack(shape):
     assert rel_err(_np(u.data[1]), qs[1]) < 1e-12
 
 
+@pytest.mark.parametrize("qr_mode", [1, 2])
+def test_qr_placement_knob(qr_mode):
+    """The QR with the walker staged in shared memory (qr_mode 1) or factored
+    in place in global memory (qr_mode 2, tuning record): both LAPACK's."""
+    from ad_afqmc_b200 import _lib
+    from ad_afqmc_b200.walkers import RHFWalkers, _dims
+
+    rng = np.random.default_rng(8)
+    W, N, no = 9, 200, 40
+    a = rng.standard_normal((W, N, no)) + 1j * rng.standard_normal((W, N, no))
+    q_ref, _ = orc.qr_restricted(a)
+    d = _dims(N, (no, no), W, "restricted")
+    t = _lib.afq_tuning()
+    t.qr_mode = qr_mode
+    _lib.set_tuning(d, t)
+    try:
+        out = RHFWalkers(a.copy()).orthonormalize()
+        got = _np(out.data)
+    finally:
+        _lib.set_tuning(d, None)
+    assert rel_err(got, q_ref) < 1e-12
+
+
 def test_qr_large_walker_global_memory_path():
     """N=300, No=60 does not fit in shared memory: the in-place global path."""
     from ad_afqmc_b200.walkers import UHFWalkers
