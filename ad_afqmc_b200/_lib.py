@@ -13,10 +13,13 @@ from typing import Optional, Sequence
 import torch
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "lib", "libafqmc_b200.so")
+# AFQ_CHECKS=1 selects the debug build (python -m ad_afqmc_b200.build --checks)
+LIB_PATH = os.path.join(_PKG, "lib", "libafqmc_b200_checks.so" if os.environ.get("AFQ_CHECKS") == "1"
+                        else "libafqmc_b200.so")
 
 AFQ_OK = 0
 AFQ_ERR_TIMEOUT = 8
+AFQ_ERR_BOUNDS = 9
 AFQ_RESTRICTED, AFQ_UNRESTRICTED = 0, 1
 AFQ_TRIAL_RHF, AFQ_TRIAL_UHF = 0, 1
 AFQ_FP64, AFQ_MIXED, AFQ_MIXED_HI = 0, 1, 2

@@ -22,11 +22,10 @@ Knobs (0 = the built-in rule):
                     alternates the direction over the walkers from one launch
                     to the next (each starts where the previous one ended, on
                     data still in L2), 1 always runs forward
-  prop_chunk        1: the propagator accumulates its whole K in one TMEM
-                    chain instead of FP32 round-to-nearest sums of four-block
-                    chunks (frees shared memory for a deeper pipeline: 85 ->
-                    78 us per launch at N=200, W=512, with a block-energy
-                    deviation from FP64 of 0.044 instead of 0.039 mHa).  Not
+  prop_chunk        2: the propagator sums its K in FP32 round-to-nearest
+                    chunks of four 64-wide blocks (shared-memory staging, two
+                    operand stages) instead of the built-in single TMEM chain
+                    (four stages: 87 -> 79 us per launch at N=200, W=512).  Not
                     searched: it changes results beyond the last bits
   grid_cap          CTAs of the persistent kernels (a batch-level knob: a
                     solve alone never gains from fewer CTAs, but overlapping

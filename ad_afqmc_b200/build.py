@@ -20,6 +20,7 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libafqmc_b200.so")
+LIB_CHECKS = os.path.join(LIBDIR, "libafqmc_b200_checks.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -44,33 +45,40 @@ def _deps_mtime():
     return max(os.path.getmtime(p) for p in paths)
 
 
-def _compile(src: str, force: bool) -> str:
-    obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+def _compile(src: str, force: bool, checks: bool = False) -> str:
+    bdir = BUILD + ("_checks" if checks else "")
+    obj = os.path.join(bdir, os.path.basename(src)[:-3] + ".o")
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= _deps_mtime():
         return obj
-    cmd = [nvcc(), *ARCH, *FLAGS, "-c", src, "-o", obj]
+    cmd = [nvcc(), *ARCH, *FLAGS, *(["-DAFQ_CHECKS"] if checks else []), "-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stderr}")
     return obj
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, checks: bool = False) -> str:
+    """Build the library; ``checks`` builds the debug variant
+    (libafqmc_b200_checks.so, -DAFQ_CHECKS: host pointers rejected before any
+    launch, out-of-range GEMM tiles reported as AFQ_ERR_BOUNDS), which
+    ``_lib`` loads when the environment sets AFQ_CHECKS=1."""
+    bdir = BUILD + ("_checks" if checks else "")
+    lib_path = LIB_CHECKS if checks else LIB
+    os.makedirs(bdir, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
-        objs = list(ex.map(lambda s: _compile(s, force), srcs))
+        objs = list(ex.map(lambda s: _compile(s, force, checks), srcs))
     newest = max(os.path.getmtime(o) for o in objs)
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-cudart=static"]
+    if force or not os.path.exists(lib_path) or os.path.getmtime(lib_path) < newest:
+        cmd = [nvcc(), *ARCH, "-shared", "-o", lib_path, *objs, "-cudart=static"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
     if verbose:
-        print(LIB)
-    return LIB
+        print(lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
+    build(force="--force" in sys.argv, verbose=True, checks="--checks" in sys.argv)

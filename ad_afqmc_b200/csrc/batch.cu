@@ -27,7 +27,7 @@ struct afq_batch {
   OvlpArgs* ovlp = nullptr;
   WeightArgs* weight = nullptr;
   BlockMap m_green{}, m_prep{}, m_wt[2]{}, m_ovlp{};
-  size_t green_smem = 0, gj_smem = 0, theta_smem = 0;
+  size_t green_smem = 0, gj_smem = 0;
 };
 
 namespace {
@@ -130,7 +130,6 @@ int afq_batch_create(int32_t n, const afq_dims* dims, const void* const* prepare
     gb += l.W * l.ns;
     b->green_smem = std::max(b->green_smem, green_smem_bytes(l.nomax));
     b->gj_smem = std::max(b->gj_smem, gj_smem_bytes(l.nomax));
-    b->theta_smem = std::max(b->theta_smem, green_theta_smem_bytes(l.nomax));
     gj[f] = GjArgs{l.W, l.no[0], l.ns > 1 ? l.no[1] : 0, l.nomax * (l.nomax | 1), Wk[f] + l.w_s,
                    (long long)l.nomax * l.nomax, Wk[f] + l.w_wscal};
     PrepArgs p{};
@@ -227,7 +226,7 @@ int afq_batch_propagate_constrained(afq_batch* b, int32_t step, int32_t green_cu
   if (!green_current) {
     AFQ_B(launch_green_grouped(b->green, b->m_green, 1, b->green_smem, st));
     AFQ_B(launch_gj_grouped(b->gj, b->m_green, b->gj_smem, st));
-    AFQ_B(launch_green_grouped(b->green, b->m_green, 2, b->theta_smem, st));
+    AFQ_B(launch_green_grouped(b->green, b->m_green, 2, b->green_smem, st));
   }
   int rc = umma_batch_fb(b->umma, st);
   if (rc != AFQ_OK) return rc;
@@ -242,7 +241,7 @@ int afq_batch_propagate_constrained(afq_batch* b, int32_t step, int32_t green_cu
   // new overlaps, the next step's force-bias operand, weights
   AFQ_B(launch_green_grouped(b->green, b->m_green, 1, b->green_smem, st));
   AFQ_B(launch_gj_grouped(b->gj, b->m_green, b->gj_smem, st));
-  AFQ_B(launch_green_grouped(b->green, b->m_green, 2, b->theta_smem, st));
+  AFQ_B(launch_green_grouped(b->green, b->m_green, 2, b->green_smem, st));
   AFQ_B(launch_ovlp_grouped(b->ovlp, b->m_ovlp, st));
   AFQ_B(launch_weight_grouped(b->weight, b->n, st));
 #undef AFQ_B

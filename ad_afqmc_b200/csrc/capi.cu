@@ -18,6 +18,23 @@ inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 
     if (_e != cudaSuccess) return AFQ_ERR_CUDA; \
   } while (0)
 
+// Debug builds (-DAFQ_CHECKS, libafqmc_b200_checks.so): every pointer an
+// entry point dereferences on the device must be device (or managed) memory;
+// a host pointer is rejected with AFQ_ERR_ARG before anything is launched.
+inline bool device_ptr_ok(const void* p) {
+#ifdef AFQ_CHECKS
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+#else
+  (void)p;
+  return true;
+#endif
+}
+
 int check_common(const afq_dims* d, Layout& L, const void* prepared, void* work,
                  size_t work_bytes) {
   int rc = make_layout(d, L);
@@ -25,15 +42,18 @@ int check_common(const afq_dims* d, Layout& L, const void* prepared, void* work,
   if (!prepared || !work) return AFQ_ERR_NULL;
   if (!aligned16(prepared) || !aligned16(work)) return AFQ_ERR_ALIGN;
   if (work_bytes < (size_t)L.work * sizeof(double)) return AFQ_ERR_WORKSPACE;
+  if (!device_ptr_ok(prepared) || !device_ptr_ok(work)) return AFQ_ERR_ARG;
   return AFQ_OK;
 }
 
 int check_walkers(const Layout& L, const double* const w[2]) {
   if (!w || !w[0]) return AFQ_ERR_NULL;
   if (!aligned16(w[0])) return AFQ_ERR_ALIGN;
+  if (!device_ptr_ok(w[0])) return AFQ_ERR_ARG;
   if (L.ns == 2) {
     if (!w[1]) return AFQ_ERR_NULL;
     if (!aligned16(w[1])) return AFQ_ERR_ALIGN;
+    if (!device_ptr_ok(w[1])) return AFQ_ERR_ARG;
   }
   return AFQ_OK;
 }
@@ -102,6 +122,7 @@ const char* afq_status_string(int status) {
     case AFQ_ERR_ARG: return "argument out of range";
     case AFQ_ERR_LIMIT: return "size exceeds the fixed static scratch capacity";
     case AFQ_ERR_TIMEOUT: return "a device-side wait timed out; results since the last check are invalid";
+    case AFQ_ERR_BOUNDS: return "a device-side bounds check failed (debug build); results are invalid";
     default: return "unknown status";
   }
 }
@@ -275,6 +296,9 @@ int afq_propagate_constrained(const afq_dims* d, const void* prepared, afq_state
   if (!s || !fields || !s->weights || !s->overlaps || !s->scalars) return AFQ_ERR_NULL;
   const double* const wc[2] = {s->walkers[0], s->walkers[1]};
   if ((rc = check_walkers(L, wc)) != AFQ_OK) return rc;
+  if (!device_ptr_ok(fields) || !device_ptr_ok(s->weights) || !device_ptr_ok(s->overlaps) ||
+      !device_ptr_ok(s->scalars))
+    return AFQ_ERR_ARG;
   const double* P = static_cast<const double*>(prepared);
   double* Wk = static_cast<double*>(work);
   cudaStream_t st = as_stream(stream);

@@ -125,24 +125,10 @@ __device__ double2 gauss_jordan_cta(double2* S, double2* colk, int* perm, double
   return det;
 }
 
-// Stage buffer (double2 units) of the Theta-only variant: walker rows of one
-// chunk, also holding the chunk's Theta rows once they have been consumed
-__host__ __device__ inline int theta_stage_buf(int no) {
-  const int sd = 2 * no + ((20 - (2 * no) % 16) % 16);
-  const int a = kRowChunk * (sd / 2), b = kRowChunk * (no + 1);
-  return a > b ? a : b;
-}
-
 // mode 0: the whole computation; 1: S = C^T W only, into a.sbuf; 2: Theta
 // and its outputs from S^-1 in a.sbuf (the inverse and det by gj_kernel).
-// THETA_ONLY (mode 2): no trial-row buffers, and each chunk's transposed
-// Theta rows are staged in the chunk's own walker-row buffer after its
-// products are done, so the CTA needs about 70 KB of shared memory instead of
-// 110 KB (three CTAs per SM); the arithmetic is the same.
-template <bool THETA_ONLY>
 __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, int sct) {
   extern __shared__ double2 sm[];
-  if (THETA_ONLY) mode = 2;
   const GreenSector& S_ = a.sec[sct];
   const int N = a.N, no = S_.no, tid = threadIdx.x;
   constexpr int T = kGreenThreads;
@@ -155,10 +141,10 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
   // take the minimum two shared-memory wavefronts
   const int nc2_ = 2 * no;
   const int sd = nc2_ + ((20 - nc2_ % 16) % 16);
-  const int sbuf_ = THETA_ONLY ? theta_stage_buf(no) : kRowChunk * (sd / 2);  // double2 per buffer
+  const int sbuf_ = kRowChunk * (sd / 2);  // double2 per buffer
   double2* stage = colk + 64;                                            // 2 x sbuf_
   double* moc = reinterpret_cast<double*>(stage + 2 * sbuf_);             // 2 x kRowChunk*no
-  double2* tstage = THETA_ONLY ? nullptr : reinterpret_cast<double2*>(moc + 2 * kRowChunk * no);
+  double2* tstage = reinterpret_cast<double2*>(moc + 2 * kRowChunk * no);
   const int ts = no + 1;  // padded row stride of tstage (conflict-free column reads)
   __shared__ double red[2 * (T / 32)];
   __shared__ int perm[64];
@@ -282,7 +268,6 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
     cp_async_wait1();
     __syncthreads();
     const double* stageD = reinterpret_cast<const double*>(stage + (c & 1) * sbuf_);
-    double2* tst = THETA_ONLY ? stage + (c & 1) * sbuf_ : tstage;
     // Theta rows (N x 2No real) = W rows (N x 2No) times the real form of
     // S^-1: R[2i][2j] = R[2i+1][2j+1] = Re s_ij, R[2i][2j+1] = Im s_ij,
     // R[2i+1][2j] = -Im s_ij, generated in the B fragments
@@ -318,7 +303,6 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
           }
         }
       }
-      if (THETA_ONLY) __syncthreads();  // the chunk's walker rows are consumed: reuse the buffer
 #pragma unroll
       for (int sl = 0; sl < 2; ++sl) {
         const int ni = warp + sl * 8;
@@ -328,7 +312,7 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
           const int r = ri * 8 + (lane >> 2), j = ni * 4 + (lane & 3);
           if (ri < rtiles && r < rows && j < no) {
             const double2 sv = make_double2(tacc[sl][ri][0], tacc[sl][ri][1]);
-            tst[r * ts + j] = sv;
+            tstage[r * ts + j] = sv;
             if (th) th[(long long)(p0 + r) * no + j] = sv;
             if (S_.rh1) {
               const double h = S_.rh1[(long long)j * N + p0 + r];
@@ -343,7 +327,7 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
     if (go || gre || gb || tb) {
       for (int e = tid; e < rows * no; e += T) {
         const int j = e / rows, r = e - (e / rows) * rows;
-        const double2 v = tst[r * ts + j];
+        const double2 v = tstage[r * ts + j];
         if (go) go[(long long)j * N + p0 + r] = v;
         if (gre) {
           gre[(long long)j * N + p0 + r] = v.x;
@@ -545,24 +529,14 @@ __device__ __forceinline__ void gj_body(int W, int no0, int no1, double* sbuf, l
 }
 
 __global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int mode) {
-  green_body<false>(a, mode, blockIdx.x, blockIdx.y);
-}
-
-__global__ void __launch_bounds__(kGreenThreads, 3) green_theta_kernel(GreenArgs a) {
-  green_body<true>(a, 2, blockIdx.x, blockIdx.y);
+  green_body(a, mode, blockIdx.x, blockIdx.y);
 }
 
 __global__ void __launch_bounds__(kGreenThreads) green_kernel_grouped(const GreenArgs* A, BlockMap m,
                                                                       int mode) {
   int local;
   const GreenArgs& a = A[block_owner(m, blockIdx.x, local)];
-  green_body<false>(a, mode, local % a.W, local / a.W);
-}
-
-__global__ void __launch_bounds__(kGreenThreads, 3) green_theta_grouped(const GreenArgs* A, BlockMap m) {
-  int local;
-  const GreenArgs& a = A[block_owner(m, blockIdx.x, local)];
-  green_body<true>(a, 2, local % a.W, local / a.W);
+  green_body(a, mode, local % a.W, local / a.W);
 }
 
 __global__ void __launch_bounds__(kGreenThreads, 4)
@@ -614,20 +588,9 @@ size_t green_smem_bytes(int nomax) {
 // two row-padded copies of S (row stride nomax | 1) and two scaled pivot rows
 size_t gj_smem_bytes(int nomax) { return (2 * size_t(nomax) * (nomax | 1) + 128) * sizeof(double2); }
 
-size_t green_theta_smem_bytes(int nomax) {
-  return (size_t(nomax) * nomax + 64 + 2 * size_t(theta_stage_buf(nomax))) * sizeof(double2);
-}
-
 cudaError_t launch_green_grouped(const GreenArgs* args, const BlockMap& m, int mode, size_t smem,
                                  cudaStream_t st) {
   ProfScope ps(K_GREEN, st);
-  if (mode == 2) {
-    cudaError_t e = cudaFuncSetAttribute(green_theta_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    green_theta_grouped<<<m.start[m.n], kGreenThreads, smem, st>>>(args, m);
-    return cudaGetLastError();
-  }
   cudaError_t e = cudaFuncSetAttribute(green_kernel_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
@@ -677,11 +640,7 @@ cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   gj_kernel<<<grid, kGreenThreads, gsmem, st>>>(a.W, a.sec[0].no, a.ns > 1 ? a.sec[1].no : 0,
                                                 a.sbuf, a.sstride, bstride, a.wscal);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const size_t tsmem = green_theta_smem_bytes(nomax);
-  if ((e = cudaFuncSetAttribute(green_theta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)tsmem)) != cudaSuccess)
-    return e;
-  green_theta_kernel<<<grid, kGreenThreads, tsmem, st>>>(a);
+  green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 2);
   return cudaGetLastError();
 }
 

@@ -508,10 +508,12 @@ int prop_launch(const Layout& L, const double* prep, double* work, int s, int nc
   P.epi.bt_bs = btbs;
   P.epi.wout = wout;
   P.s.ngroups = 2;
-  // K in chunks of four 64-wide blocks summed in FP32 round-to-nearest through
-  // a shared-memory row per TMEM lane, or (prop_chunk = 1) the whole K in one
-  // TMEM chain, which frees that staging for deeper operand pipelines
-  const bool one_chain = L.tune.prop_chunk == 1;
+  // The whole K (2N) in one TMEM chain, which leaves the shared memory to the
+  // operand pipeline (four stages at N = 200: 87 -> 79 us per launch, and
+  // 469 -> 335 us at N = 300; block energies within 2e-5 Ha of FP64 either
+  // way), or (prop_chunk = 2) chunks of four 64-wide K blocks summed in FP32
+  // round-to-nearest through a shared-memory row per TMEM lane
+  const bool one_chain = L.tune.prop_chunk != 2;
   P.s.kc = one_chain ? 0 : 4;
   const size_t ex = one_chain ? 0 : umma_chunk_stage_bytes(BN);
   // the propagator's epilogue (FP32 accumulator update, next operand pieces)

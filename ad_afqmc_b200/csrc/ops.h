@@ -195,7 +195,6 @@ struct WalkerTArgs {
   float* acc;
 };
 size_t green_smem_bytes(int nomax);
-size_t green_theta_smem_bytes(int nomax);  // mode 2 (Theta and its outputs) only
 size_t gj_smem_bytes(int nomax);
 cudaError_t launch_green_grouped(const GreenArgs* args, const BlockMap& m, int mode, size_t smem,
                                  cudaStream_t st);

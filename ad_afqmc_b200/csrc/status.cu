@@ -60,7 +60,7 @@ int afq_check_status(const afq_dims* d, void* work, size_t work_bytes, void* str
   if (host == 0) return AFQ_OK;
   if (cudaMemsetAsync(flag, 0, sizeof(int), st) != cudaSuccess) return AFQ_ERR_CUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return AFQ_ERR_CUDA;
-  return AFQ_ERR_TIMEOUT;
+  return host == 2 ? AFQ_ERR_BOUNDS : AFQ_ERR_TIMEOUT;
 }
 
 int afq_status_flag(const afq_dims* d, void* work, size_t work_bytes, int32_t** flag) {

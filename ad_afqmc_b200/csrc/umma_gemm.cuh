@@ -207,6 +207,15 @@ __device__ __forceinline__ void umma_body(const Src& src) {
     const int etiles = S.batch * S.ksplit * S.mt * S.nt;
     const int tile = S.reverse ? etiles - 1 - local : local;
     TileAt t;
+#ifdef AFQ_CHECKS
+    // debug builds: a tile outside its GEMM (a corrupt work list) is reported
+    // (flag value 2) and skipped by every role alike (KB = 0)
+    if (local < 0 || local >= etiles) {
+      atomicExch(S.err, 2);
+      t.z = t.mti = t.nti = t.b = t.k0 = t.KB = 0;
+      return t;
+    }
+#endif
     t.nti = tile % S.nt;
     const int rest = tile / S.nt;
     t.mti = rest % S.mt;
@@ -261,6 +270,7 @@ __device__ __forceinline__ void umma_body(const Src& src) {
         const UmmaShape& S = P.s;
         const TileAt tl = locate(S, local);
         const int KB = tl.KB;
+        if (KB == 0) continue;  // (debug builds: a tile skipped by every role)
         const int kc = S.kc > 0 ? S.kc : KB;
         bool ok = true;
         for (int c0 = 0; c0 < KB && ok; c0 += kc, ++it) {
@@ -311,6 +321,7 @@ __device__ __forceinline__ void umma_body(const Src& src) {
       const UmmaShape& S = P.s;
       const TileAt tl = locate(S, local);
       const int KB = tl.KB;
+      if (KB == 0) continue;
       const int kc = S.kc > 0 ? S.kc : KB;
       const int nch = (KB + kc - 1) / kc;
       for (int ch = 0; ch < nch; ++ch, ++it) {

@@ -43,7 +43,8 @@ typedef enum afq_status {
   AFQ_ERR_ALIGN = 5,      /* a pointer is not 16-byte aligned             */
   AFQ_ERR_ARG = 6,        /* an enum/flag argument is out of range        */
   AFQ_ERR_LIMIT = 7,      /* size beyond a fixed (static) scratch capacity */
-  AFQ_ERR_TIMEOUT = 8     /* a bounded device-side wait ran out (afq_check_status) */
+  AFQ_ERR_TIMEOUT = 8,    /* a bounded device-side wait ran out (afq_check_status) */
+  AFQ_ERR_BOUNDS = 9      /* debug builds: a device-side bounds check failed */
 } afq_status;
 
 enum { AFQ_RESTRICTED = 0, AFQ_UNRESTRICTED = 1 };      /* walker_type  */
@@ -290,8 +291,10 @@ typedef struct afq_tuning {
   int32_t prop_epi_groups; /* epilogue warpgroups of the tensor-core propagator: 1 to 3    */
   int32_t prop_order;  /* propagator tile order: 0 alternate direction per launch (the     */
                        /* walkers last read stay in L2 for the next launch), 1 forward     */
-  int32_t prop_chunk;  /* propagator K accumulation: 0 chunks of four 64-wide K blocks     */
-                       /* summed in FP32 round-to-nearest, 1 the whole K in one chain     */
+  int32_t prop_chunk;  /* propagator K accumulation: 0 built-in (the whole K in one TMEM  */
+                       /* chain), 1 the whole K in one chain, 2 chunks of four 64-wide K   */
+                       /* blocks summed in FP32 round-to-nearest (less shared memory left  */
+                       /* for the operand pipeline)                                         */
   int32_t qr_mode;     /* QR of the walkers: 0 built-in choice, 1 walker in shared memory   */
                        /* (when it fits), 2 in place in global memory                       */
   int32_t reserved[5];
