@@ -84,11 +84,12 @@ class afq_tuning(C.Structure):
         ("prop_order", C.c_int32),
         ("prop_chunk", C.c_int32),
         ("qr_mode", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("vhs_chunk", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
     KNOBS = ("fb_splitk", "fb_bn", "vhs_bn", "exch_bn", "f64_exch_bn", "max_stages", "grid_cap",
-             "prop_epi_groups", "prop_order", "prop_chunk", "qr_mode")
+             "prop_epi_groups", "prop_order", "prop_chunk", "qr_mode", "vhs_chunk")
 
     def as_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k in self.KNOBS}

@@ -27,6 +27,11 @@ Knobs (0 = the built-in rule):
                     operand stages) instead of the built-in single TMEM chain
                     (four stages: 87 -> 79 us per launch at N=200, W=512).  Not
                     searched: it changes results beyond the last bits
+  vhs_chunk         2: the VHS GEMM sums its K (= Nchol) in FP32 chunks of
+                    four 64-wide blocks instead of the built-in single TMEM
+                    chain per accumulator group (364 vs 276 us per launch at
+                    N=200, G=1000, W=512).  Not searched: it changes results
+                    beyond the last bits
   grid_cap          CTAs of the persistent kernels (a batch-level knob: a
                     solve alone never gains from fewer CTAs, but overlapping
                     fragments can; ``tune_batch`` sweeps it for a whole batch)

@@ -194,6 +194,7 @@ inline int make_layout(const afq_dims* d, Layout& L, const afq_tuning* record = 
   if (T.prop_order < 0 || T.prop_order > 1) return AFQ_ERR_ARG;
   if (T.prop_chunk < 0 || T.prop_chunk > 2) return AFQ_ERR_ARG;
   if (T.qr_mode < 0 || T.qr_mode > 2) return AFQ_ERR_ARG;
+  if (T.vhs_chunk < 0 || T.vhs_chunk > 2) return AFQ_ERR_ARG;
   if (T.vhs_bn != 0 && T.vhs_bn != 64 && T.vhs_bn != 128) return AFQ_ERR_ARG;
   if (T.fb_splitk > 0) L.splitk = T.fb_splitk;
   for (int s = 0; s < 2; ++s) {

@@ -641,10 +641,15 @@ int vhs_launch(const Layout& L, const double* prep, double* work, cudaStream_t s
   P.epi.N = L.N;
   P.epi.ld = L.Kv;
   P.epi.wstride = (long long)L.N * L.Kv;
-  // K = G accumulates in chunks of 4 K blocks, the hi x hi product apart
+  // K = G in one TMEM chain per accumulator group (the hi x hi product apart),
+  // which leaves the shared memory to four operand stages (364 -> 276 us per
+  // launch at N = 200, G = 1000, W = 512; block energies 7.8e-6 Ha from FP64),
+  // or (vhs_chunk = 2) in chunks of four 64-wide K blocks summed in FP32
+  // round-to-nearest through a shared-memory row per TMEM lane (5.0e-6 Ha)
   P.s.ngroups = 2;
-  P.s.kc = 4;
-  return run<BN>(P, umma_chunk_stage_bytes(BN), st, K_VHS, L.tune);
+  const bool one_chain = L.tune.vhs_chunk != 2;
+  P.s.kc = one_chain ? 0 : 4;
+  return run<BN>(P, one_chain ? 0 : umma_chunk_stage_bytes(BN), st, K_VHS, L.tune);
 }
 
 int mixed_vhs_gemm(const Layout& L, const double* prep, double* work, cudaStream_t st) {

@@ -74,122 +74,272 @@ __global__ void __launch_bounds__(kWeightThreads) weight_kernel_grouped(const We
 // Householder QR, LAPACK convention (zlarfg: beta = -sign(Re a) |x|,
 // tau = ((beta - ar)/beta, -ai/beta), v = x / (a - beta)), explicit Q as zung2r.
 // A is a generic pointer (shared or global memory), row stride lda (double2).
+//
+// One warp per column: warp (j mod warps) owns column j for the whole
+// factorisation.  Applying a reflector to a column is a warp-local product
+// (w_j = v^H a_j by shuffles) and update, so each reflector costs one block
+// barrier: in geqr2 the owner of column k + 1 forms the next reflector right
+// after the column received reflector k; in zung2r the owner of column i + 1
+// turns it into a column of Q just before applying reflector i to it (no
+// other warp reads column i + 1 at that step, while column i, which every
+// warp reads as the reflector, is left alone until the next step).
 // ---------------------------------------------------------------------------
-constexpr int kQrThreads = 256;
+constexpr int kQrThreads = 1024;
 
-__device__ void qr_inplace(double2* A, int lda, int N, int no, double2* tau, double* beta,
-                           double2* wv, double2* wpart, double* red, double2* scal_s) {
-  const int tid = threadIdx.x;
-  constexpr int T = kQrThreads;
-  for (int k = 0; k < no; ++k) {
-    double s = 0.0;
-    for (int p = k + 1 + tid; p < N; p += T) {
-      const double2 v = A[p * lda + k];
-      s += v.x * v.x + v.y * v.y;
-    }
-    s = block_sum(s, red);
-    if (tid == 0) {
-      const double2 al = A[k * lda + k];
-      if (s == 0.0 && al.y == 0.0) {
-        tau[k] = make_double2(0.0, 0.0);
-        beta[k] = al.x;
-        *scal_s = make_double2(1.0, 0.0);
-      } else {
-        const double b = -copysign(sqrt(al.x * al.x + al.y * al.y + s), al.x);
-        tau[k] = make_double2((b - al.x) / b, -al.y / b);
-        beta[k] = b;
-        *scal_s = cdiv(make_double2(1.0, 0.0), make_double2(al.x - b, al.y));
-      }
-    }
-    __syncthreads();
-    const double2 sc = *scal_s;
-    const double2 tk = tau[k];
-    for (int p = k + 1 + tid; p < N; p += T) A[p * lda + k] = cmul(A[p * lda + k], sc);
-    if (tid == 0) A[k * lda + k] = make_double2(1.0, 0.0);
-    __syncthreads();
-    const int nj = no - k - 1;
-    if (nj > 0 && (tk.x != 0.0 || tk.y != 0.0)) {
-      // w_j = sum_p conj(v_p) A[p][j]
-      const int nrs = T / nj;
-      if (tid < nrs * nj) {
-        const int j = k + 1 + tid % nj, rs = tid / nj;
-        double2 acc = make_double2(0.0, 0.0);
-        for (int p = k + rs; p < N; p += nrs) acc = cadd(acc, cmul(cconj(A[p * lda + k]), A[p * lda + j]));
-        wpart[tid] = acc;
-      }
-      __syncthreads();
-      for (int j = tid; j < nj; j += T) {
-        double2 acc = make_double2(0.0, 0.0);
-        for (int rs = 0; rs < nrs; ++rs) acc = cadd(acc, wpart[rs * nj + j]);
-        wv[j] = acc;
-      }
-      __syncthreads();
-      // A[p][j] -= conj(tau) v_p w_j     (H^H applied from the left)
-      const double2 ct = cconj(tk);
-      // thread -> (row offset, column) once per column; rows advance by T / nj
-      const int pstep = T / nj, j = tid % nj;
-      if (tid < pstep * nj) {
-        const double2 cw = cmul(ct, wv[j]);
-        for (int p = k + tid / nj; p < N; p += pstep) {
-          const double2 vp = A[p * lda + k];
-          A[p * lda + k + 1 + j] = csub(A[p * lda + k + 1 + j], cmul(vp, cw));
-        }
-      }
-      __syncthreads();
-    }
-    if (tid == 0) A[k * lda + k] = make_double2(beta[k], 0.0);
-    __syncthreads();
+__device__ __forceinline__ double2 warp_sum2(double2 v) {
+  return make_double2(warp_sum(v.x), warp_sum(v.y));
+}
+
+// first column > k owned by this warp
+__device__ __forceinline__ int qr_first_col(int k, int warp, int nw) {
+  return k + 1 + ((warp - (k + 1)) % nw + nw) % nw;
+}
+
+// reflector of column k from its entries k..N-1 (zlarfg); owner warp only
+__device__ void qr_reflector(double2* A, int lda, int N, int k, double2* tau, double* beta) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int p = k + 1 + lane; p < N; p += 32) {
+    const double2 v = A[p * lda + k];
+    s += v.x * v.x + v.y * v.y;
   }
-  // explicit Q (zung2r)
-  for (int i = no - 1; i >= 0; --i) {
-    const double2 ti = tau[i];
-    if (i < no - 1) {
-      if (tid == 0) A[i * lda + i] = make_double2(1.0, 0.0);
-      __syncthreads();
-      const int nj = no - i - 1;
-      const int nrs = T / nj;
-      if (tid < nrs * nj) {
-        const int j = i + 1 + tid % nj, rs = tid / nj;
-        double2 acc = make_double2(0.0, 0.0);
-        for (int p = i + rs; p < N; p += nrs) acc = cadd(acc, cmul(cconj(A[p * lda + i]), A[p * lda + j]));
-        wpart[tid] = acc;
-      }
-      __syncthreads();
-      for (int j = tid; j < nj; j += T) {
-        double2 acc = make_double2(0.0, 0.0);
-        for (int rs = 0; rs < nrs; ++rs) acc = cadd(acc, wpart[rs * nj + j]);
-        wv[j] = acc;
-      }
-      __syncthreads();
-      const int pstep = T / nj, j = tid % nj;
-      if (tid < pstep * nj) {
-        const double2 cw = cmul(ti, wv[j]);
-        for (int p = i + tid / nj; p < N; p += pstep) {
-          const double2 vp = A[p * lda + i];
-          A[p * lda + i + 1 + j] = csub(A[p * lda + i + 1 + j], cmul(vp, cw));
-        }
-      }
-      __syncthreads();
-    }
-    const double2 mt = make_double2(-ti.x, -ti.y);
-    for (int p = i + 1 + tid; p < N; p += T) A[p * lda + i] = cmul(A[p * lda + i], mt);
-    for (int p = tid; p < i; p += T) A[p * lda + i] = make_double2(0.0, 0.0);
-    if (tid == 0) A[i * lda + i] = make_double2(1.0 - ti.x, -ti.y);
-    __syncthreads();
+  s = warp_sum(s);
+  const double2 al = A[k * lda + k];
+  double2 tk, sc;
+  double b;
+  if (s == 0.0 && al.y == 0.0) {
+    tk = make_double2(0.0, 0.0);
+    b = al.x;
+    sc = make_double2(1.0, 0.0);
+  } else {
+    b = -copysign(sqrt(al.x * al.x + al.y * al.y + s), al.x);
+    tk = make_double2((b - al.x) / b, -al.y / b);
+    sc = cdiv(make_double2(1.0, 0.0), make_double2(al.x - b, al.y));
+  }
+  for (int p = k + 1 + lane; p < N; p += 32) A[p * lda + k] = cmul(A[p * lda + k], sc);
+  __syncwarp();
+  if (lane == 0) {
+    tau[k] = tk;
+    beta[k] = b;
+    A[k * lda + k] = make_double2(b, 0.0);  // R's diagonal; v_k = 1 is implicit
   }
 }
 
+// a_j -= c v (v^H a_j) over rows k..N-1, v read from vk (v_k = 1 implicit
+// when `unit`, else vk[k] itself); one warp
+__device__ __forceinline__ void qr_apply(double2* A, int lda, int N, int k, int j, const double2* vk,
+                                         int vstride, bool unit, double2 c) {
+  const int lane = threadIdx.x & 31;
+  double2 w = make_double2(0.0, 0.0);
+  for (int p = k + lane; p < N; p += 32) {
+    const double2 vp = (unit && p == k) ? make_double2(1.0, 0.0) : vk[p * vstride];
+    w = cadd(w, cmul(cconj(vp), A[p * lda + j]));
+  }
+  const double2 cw = cmul(c, warp_sum2(w));
+  for (int p = k + lane; p < N; p += 32) {
+    const double2 vp = (unit && p == k) ? make_double2(1.0, 0.0) : vk[p * vstride];
+    A[p * lda + j] = csub(A[p * lda + j], cmul(vp, cw));
+  }
+}
+
+// column i of Q from reflector i stored in it: -tau v below, 1 - tau on and
+// 0 above the diagonal; owner warp only
+__device__ __forceinline__ void qr_q_column(double2* A, int lda, int N, int i, double2 ti) {
+  const int lane = threadIdx.x & 31;
+  for (int p = lane; p < N; p += 32)
+    A[p * lda + i] = p < i ? make_double2(0.0, 0.0)
+                           : (p == i ? make_double2(1.0 - ti.x, -ti.y)
+                                     : cmul(make_double2(-ti.x, -ti.y), A[p * lda + i]));
+}
+
+__device__ void qr_inplace(double2* A, int lda, int N, int no, double2* tau, double* beta) {
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // ---- geqr2: R above the diagonal, reflectors below ----------------------
+  if (warp == 0) qr_reflector(A, lda, N, 0, tau, beta);
+  __syncthreads();
+  for (int k = 0; k + 1 < no; ++k) {
+    const double2 ct = cconj(tau[k]);  // H^H applied from the left
+    const bool active = ct.x != 0.0 || ct.y != 0.0;
+    for (int j = qr_first_col(k, warp, nw); j < no; j += nw) {
+      if (active) qr_apply(A, lda, N, k, j, A + k, lda, true, ct);
+      if (j == k + 1) {
+        __syncwarp();
+        qr_reflector(A, lda, N, k + 1, tau, beta);
+      }
+    }
+    __syncthreads();
+  }
+  // ---- zung2r: explicit Q, reflectors applied last to first ---------------
+  for (int i = no - 2; i >= 0; --i) {
+    const double2 ti = tau[i];
+    const bool active = ti.x != 0.0 || ti.y != 0.0;
+    for (int j = qr_first_col(i, warp, nw); j < no; j += nw) {
+      if (j == i + 1) {
+        qr_q_column(A, lda, N, j, tau[j]);
+        __syncwarp();
+      }
+      if (active) qr_apply(A, lda, N, i, j, A + i, lda, true, ti);
+    }
+    __syncthreads();
+  }
+  if (warp == 0) qr_q_column(A, lda, N, 0, tau[0]);
+  __syncthreads();
+}
+
+// ---- the same factorisation with each warp's column rows in registers ----
+// Lane l holds rows r0 + l + 32 t (t < RPL) of the column it works on, where
+// r0 is the reflector's first row; N <= 32 RPL.  All RPL loads of a column are
+// in flight together and the product and update run on registers, so a
+// column step costs one round of loads, the shuffles and one round of stores.
+template <int RPL>
+__device__ __forceinline__ void rcol_load(const double2* A, int lda, int N, int r0, int j,
+                                          double2 (&a)[RPL]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int p = r0 + lane + 32 * t;
+    a[t] = p < N ? A[p * lda + j] : make_double2(0.0, 0.0);
+  }
+}
+
+template <int RPL>
+__device__ __forceinline__ void rcol_store(double2* A, int lda, int N, int r0, int j,
+                                           const double2 (&a)[RPL]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    const int p = r0 + lane + 32 * t;
+    if (p < N) A[p * lda + j] = a[t];
+  }
+}
+
+// a -= c v (v^H a); rows beyond N hold zeros in both
+template <int RPL>
+__device__ __forceinline__ void rcol_reflect(double2 (&a)[RPL], const double2 (&v)[RPL], double2 c) {
+  double2 w0 = make_double2(0.0, 0.0), w1 = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) {
+    if (t & 1)
+      w1 = cadd(w1, cmul(cconj(v[t]), a[t]));
+    else
+      w0 = cadd(w0, cmul(cconj(v[t]), a[t]));
+  }
+  const double2 cw = cmul(c, warp_sum2(cadd(w0, w1)));
+#pragma unroll
+  for (int t = 0; t < RPL; ++t) a[t] = csub(a[t], cmul(v[t], cw));
+}
+
+// reflector k (zlarfg) of a column held from row k - d: pivot in lane d, t = 0
+template <int RPL>
+__device__ __forceinline__ void rcol_reflector(double2 (&a)[RPL], int d, int k, double2* tau,
+                                               double* beta) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+#pragma unroll
+  for (int t = 0; t < RPL; ++t)
+    if (t > 0 || lane > d) s += a[t].x * a[t].x + a[t].y * a[t].y;
+  s = warp_sum(s);
+  const double2 al = make_double2(__shfl_sync(0xffffffffu, a[0].x, d), __shfl_sync(0xffffffffu, a[0].y, d));
+  double2 tk, sc;
+  double b;
+  if (s == 0.0 && al.y == 0.0) {
+    tk = make_double2(0.0, 0.0);
+    b = al.x;
+    sc = make_double2(1.0, 0.0);
+  } else {
+    b = -copysign(sqrt(al.x * al.x + al.y * al.y + s), al.x);
+    tk = make_double2((b - al.x) / b, -al.y / b);
+    sc = cdiv(make_double2(1.0, 0.0), make_double2(al.x - b, al.y));
+  }
+#pragma unroll
+  for (int t = 0; t < RPL; ++t)
+    if (t > 0 || lane > d) a[t] = cmul(a[t], sc);
+  if (lane == d) a[0] = make_double2(b, 0.0);
+  if (lane == 0) {
+    tau[k] = tk;
+    beta[k] = b;
+  }
+}
+
+// the reflector's rows r0 + l + 32 t (v_r0 = 1) into registers
+template <int RPL>
+__device__ __forceinline__ void rcol_vector(const double2* A, int lda, int N, int r0,
+                                            double2 (&v)[RPL]) {
+  rcol_load<RPL>(A, lda, N, r0, r0, v);
+  if ((threadIdx.x & 31) == 0) v[0] = make_double2(1.0, 0.0);
+}
+
+template <int RPL>
+__device__ void qr_inplace_reg(double2* A, int lda, int N, int no, double2* tau, double* beta) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double2 v[RPL], a[RPL];
+  // ---- geqr2 ----------------------------------------------------------------
+  if (warp == 0) {
+    rcol_load<RPL>(A, lda, N, 0, 0, a);
+    rcol_reflector<RPL>(a, 0, 0, tau, beta);
+    rcol_store<RPL>(A, lda, N, 0, 0, a);
+  }
+  __syncthreads();
+  for (int k = 0; k + 1 < no; ++k) {
+    const double2 ct = cconj(tau[k]);
+    const bool active = ct.x != 0.0 || ct.y != 0.0;
+    const int j0 = qr_first_col(k, warp, nw);
+    if (j0 < no) {
+      rcol_vector<RPL>(A, lda, N, k, v);
+      for (int j = j0; j < no; j += nw) {
+        rcol_load<RPL>(A, lda, N, k, j, a);
+        if (active) rcol_reflect<RPL>(a, v, ct);
+        if (j == k + 1) rcol_reflector<RPL>(a, 1, k + 1, tau, beta);
+        rcol_store<RPL>(A, lda, N, k, j, a);
+      }
+    }
+    __syncthreads();
+  }
+  // ---- zung2r ---------------------------------------------------------------
+  for (int i = no - 2; i >= 0; --i) {
+    const double2 ti = tau[i];
+    const bool active = ti.x != 0.0 || ti.y != 0.0;
+    const int j0 = qr_first_col(i, warp, nw);
+    if (j0 < no) {
+      rcol_vector<RPL>(A, lda, N, i, v);
+      for (int j = j0; j < no; j += nw) {
+        rcol_load<RPL>(A, lda, N, i, j, a);
+        if (j == i + 1) {  // column j of Q from reflector j: window starts one row above it
+          const double2 tj = tau[j];
+#pragma unroll
+          for (int t = 0; t < RPL; ++t) {
+            if (t == 0 && lane == 0) a[t] = make_double2(0.0, 0.0);
+            else if (t == 0 && lane == 1) a[t] = make_double2(1.0 - tj.x, -tj.y);
+            else a[t] = cmul(make_double2(-tj.x, -tj.y), a[t]);
+          }
+          for (int p = lane; p < i; p += 32) A[p * lda + j] = make_double2(0.0, 0.0);
+        }
+        if (active) rcol_reflect<RPL>(a, v, ti);
+        rcol_store<RPL>(A, lda, N, i, j, a);
+      }
+    }
+    __syncthreads();
+  }
+  if (warp == 0) {  // column 0 of Q
+    rcol_load<RPL>(A, lda, N, 0, 0, a);
+    const double2 t0 = tau[0];
+#pragma unroll
+    for (int t = 0; t < RPL; ++t)
+      a[t] = (t == 0 && lane == 0) ? make_double2(1.0 - t0.x, -t0.y) : cmul(make_double2(-t0.x, -t0.y), a[t]);
+    rcol_store<RPL>(A, lda, N, 0, 0, a);
+  }
+  __syncthreads();
+}
+
 // grid (W, ns).  use_smem: walker copied to shared memory with row stride no+1.
-__global__ void __launch_bounds__(kQrThreads)
-    qr_kernel(int N, int no0, int no1, double* w0, double* w1, int sign_fix, int use_smem,
-              double* sector_norm /* (ns, W) */) {
+// RPL > 0: register-resident columns (N <= 32 RPL, 512 threads); 0: the loop
+// form for any N (1024 threads).
+template <int RPL>
+__device__ __forceinline__ void qr_walker(int N, int no0, int no1, double* w0, double* w1,
+                                          int sign_fix, int use_smem, double* sector_norm) {
   extern __shared__ double2 qsm[];
   __shared__ double2 tau[64];
   __shared__ double beta[64];
-  __shared__ double2 wv[64];
-  __shared__ double2 wpart[kQrThreads];
-  __shared__ double red[kQrThreads / 32];
-  __shared__ double2 scal_s;
   const int w = blockIdx.x, s = blockIdx.y;
   const int no = s ? no1 : no0;
   double2* G = reinterpret_cast<double2*>(s ? w1 : w0) + (long long)w * N * no;
@@ -198,13 +348,16 @@ __global__ void __launch_bounds__(kQrThreads)
   if (use_smem) {
     lda = no + 1;
     A = qsm;
-    for (int e = threadIdx.x; e < N * no; e += kQrThreads) {
+    for (int e = threadIdx.x; e < N * no; e += blockDim.x) {
       const int p = e / no, j = e - (e / no) * no;
       A[p * lda + j] = G[e];
     }
     __syncthreads();
   }
-  qr_inplace(A, lda, N, no, tau, beta, wv, wpart, red, &scal_s);
+  if (RPL > 0)
+    qr_inplace_reg<(RPL > 0 ? RPL : 1)>(A, lda, N, no, tau, beta);
+  else
+    qr_inplace(A, lda, N, no, tau, beta);
   // prod diag R (real) and optional sign fix of column 0
   __shared__ double prod_s;
   if (threadIdx.x == 0) {
@@ -216,15 +369,30 @@ __global__ void __launch_bounds__(kQrThreads)
   __syncthreads();
   const double sg = sign_fix ? ((prod_s > 0.0) ? 1.0 : ((prod_s < 0.0) ? -1.0 : 0.0)) : 1.0;
   if (use_smem) {
-    for (int e = threadIdx.x; e < N * no; e += kQrThreads) {
+    for (int e = threadIdx.x; e < N * no; e += blockDim.x) {
       const int p = e / no, j = e - (e / no) * no;
       double2 v = A[p * lda + j];
       if (j == 0) v = cscale(v, sg);
       G[e] = v;
     }
   } else if (sign_fix) {
-    for (int p = threadIdx.x; p < N; p += kQrThreads) G[p * no] = cscale(G[p * no], sg);
+    for (int p = threadIdx.x; p < N; p += blockDim.x) G[p * no] = cscale(G[p * no], sg);
   }
+}
+
+constexpr int kQrRegThreads = 512;
+
+__global__ void __launch_bounds__(kQrThreads, 1)
+    qr_kernel(int N, int no0, int no1, double* w0, double* w1, int sign_fix, int use_smem,
+              double* sector_norm /* (ns, W) */) {
+  qr_walker<0>(N, no0, no1, w0, w1, sign_fix, use_smem, sector_norm);
+}
+
+template <int RPL>
+__global__ void __launch_bounds__(kQrRegThreads, 1)
+    qr_reg_kernel(int N, int no0, int no1, double* w0, double* w1, int sign_fix, int use_smem,
+                  double* sector_norm /* (ns, W) */) {
+  qr_walker<RPL>(N, no0, no1, w0, w1, sign_fix, use_smem, sector_norm);
 }
 
 __global__ void qr_norm_kernel(int W, int ns, int restricted, const double* sector_norm,
@@ -418,23 +586,41 @@ cudaError_t launch_weight_grouped(const WeightArgs* args, int n, cudaStream_t st
   return cudaGetLastError();
 }
 
+template <class K>
+static cudaError_t launch_qr_kernel(K kernel, int threads, dim3 grid, size_t dyn, cudaStream_t st,
+                                   const Layout& L, double* const walkers[2], int use_smem,
+                                   double* secn) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e != cudaSuccess) return e;
+  kernel<<<grid, threads, dyn, st>>>(L.N, L.no[0], L.no[1], walkers[0], L.ns == 2 ? walkers[1] : nullptr,
+                                     L.restricted ? 0 : 1, use_smem, secn);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_qr(const Layout& L, double* const walkers[2], double* norms, double* work,
                       cudaStream_t st) {
   const size_t smem = size_t(L.N) * (L.nomax + 1) * sizeof(double2);
   const int use_smem = smem <= 200 * 1024 && L.tune.qr_mode != 2;
   const size_t dyn = use_smem ? smem : 0;
-  cudaError_t e =
-      cudaFuncSetAttribute(qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-  if (e != cudaSuccess) return e;
   double* secn = work;  // (ns, W) doubles of scratch at the start of the workspace
   dim3 grid(L.W, L.ns);
+  cudaError_t e;
   {
     ProfScope ps(K_QR, st);
-    qr_kernel<<<grid, kQrThreads, dyn, st>>>(L.N, L.no[0], L.no[1], walkers[0],
-                                             L.ns == 2 ? walkers[1] : nullptr,
-                                             L.restricted ? 0 : 1, use_smem, secn);
+    const int N = L.N, T = kQrRegThreads;
+    if (N <= 32)
+      e = launch_qr_kernel(qr_reg_kernel<1>, T, grid, dyn, st, L, walkers, use_smem, secn);
+    else if (N <= 64)
+      e = launch_qr_kernel(qr_reg_kernel<2>, T, grid, dyn, st, L, walkers, use_smem, secn);
+    else if (N <= 128)
+      e = launch_qr_kernel(qr_reg_kernel<4>, T, grid, dyn, st, L, walkers, use_smem, secn);
+    else if (N <= 224)
+      e = launch_qr_kernel(qr_reg_kernel<7>, T, grid, dyn, st, L, walkers, use_smem, secn);
+    else if (N <= 320)
+      e = launch_qr_kernel(qr_reg_kernel<10>, T, grid, dyn, st, L, walkers, use_smem, secn);
+    else
+      e = launch_qr_kernel(qr_kernel, kQrThreads, grid, dyn, st, L, walkers, use_smem, secn);
   }
-  e = cudaGetLastError();
   if (e != cudaSuccess || !norms) return e;
   ProfScope ps(K_MISC, st);
   qr_norm_kernel<<<(L.W + 255) / 256, 256, 0, st>>>(L.W, L.ns, L.restricted, secn, norms);

@@ -297,7 +297,11 @@ typedef struct afq_tuning {
                        /* for the operand pipeline)                                         */
   int32_t qr_mode;     /* QR of the walkers: 0 built-in choice, 1 walker in shared memory   */
                        /* (when it fits), 2 in place in global memory                       */
-  int32_t reserved[5];
+  int32_t vhs_chunk;   /* VHS GEMM K accumulation: 0 built-in (the whole K in one TMEM      */
+                       /* chain per accumulator group), 1 the same, 2 chunks of four        */
+                       /* 64-wide K blocks summed in FP32 round-to-nearest (less shared     */
+                       /* memory left for the operand pipeline)                             */
+  int32_t reserved[4];
 } afq_tuning;
 
 int afq_set_tuning(const afq_dims* d, const afq_tuning* t);

@@ -92,3 +92,32 @@ def test_autotuner_record_is_used_and_cached(tmp_path):
         assert torch.isfinite(pd["weights"]).all()
     finally:
         _lib.set_tuning(eng.dims, None)
+
+
+@pytest.mark.parametrize("rec", [{}, {"vhs_chunk": 2}, {"prop_chunk": 2}, {"vhs_chunk": 2, "prop_chunk": 2}])
+@pytest.mark.parametrize("shape", [(48, (12, 12), 200, 8), (200, (40, 40), 1000, 4)])
+def test_step_under_accumulation_choices(rec, shape):
+    """The VHS GEMM and the propagator accumulate K in one TMEM chain by
+    default, or in FP32 round-to-nearest chunks of four K blocks (knob value
+    2): a step stays within the mixed path's 1e-4 of the oracle either way."""
+    import copy
+
+    N, nelec, G, W = shape
+    sys_ = make_system(N, nelec, G, seed=12, trial="rhf", chol_scale=0.25)
+    walkers = near_trial_walkers(np.random.default_rng(4), sys_.mo_coeff, W, eps=0.1)
+    fields = np.random.default_rng(5).standard_normal((W, G))
+    o_trial, o_ham, o_wave, o_prop = oracle_system(sys_, "restricted", 0.005)
+    o_prop.n_walkers = W
+    o_pd = o_prop.init_prop_data(o_trial, o_wave, o_ham, init_walkers=copy.deepcopy(walkers))
+    o_pd = o_prop.propagate_constrained(o_trial, o_ham, o_pd, fields, o_wave)
+    d_trial, d_ham, d_wave, d_prop, _ = device_system(sys_, "restricted", 0.005, W, precision="mixed")
+    eng = d_prop.engine(d_ham, d_trial, d_wave)
+    try:
+        _lib.set_tuning(eng.dims, _lib.afq_tuning.from_dict(rec) if rec else None)
+        eng.ensure_workspace()
+        d_pd = d_prop.init_prop_data(d_trial, d_wave, d_ham, 0, init_walkers=RHFWalkers(walkers.copy()))
+        d_pd = d_prop.propagate_constrained(d_trial, d_ham, d_pd, fields, d_wave)
+        got = d_pd["walkers"].data.cpu().numpy()
+    finally:
+        _lib.set_tuning(eng.dims, None)
+    assert rel_err(got, o_pd["walkers"]) < 1e-4
