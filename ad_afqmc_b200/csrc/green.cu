@@ -381,17 +381,25 @@ __device__ __forceinline__ int gj_pivot(double2 v0, double2 v1, bool ok0, bool o
 }
 
 // Gauss-Jordan inverse and det of S = C^T W held in sbuf, one CTA per
-// (walker, sector), in place, with one block barrier per elimination step
-// (partial pivoting, pivot = largest |re|+|im| in the column).
+// (walker, sector), in place in one shared-memory copy of S, with one block
+// barrier per elimination step (partial pivoting, pivot = largest |re|+|im|
+// in the column).
 //  * Rows are never swapped: the pivot row r_k of step k stays in place and
 //    the inverse is unscrambled once at the end, S^-1[i][r_k] = X[r_i][k].
-//  * Step k reads buffer k & 1 and writes the other, so nothing is read after
-//    it was overwritten within a step.  Rows are stored with an odd stride
-//    (ld = no | 1 double2), so a warp reading a column hits distinct banks.
-//  * During step k warp 0 computes the new pivot column k+1, its pivot (over
-//    the rows not yet used), the reciprocal and the scaled new pivot row,
-//    which every thread reads in step k+1; warps 1..7 update all other
-//    elements.  det = product of the pivots times the permutation's sign.
+//  * Pivot rows are scaled lazily: row r_k keeps its unscaled values U (the
+//    true row is U / p_k).  Every later update of that row has the same form
+//    on U (the update is linear in the row), so no thread writes row r_k
+//    during step k, and each thread reads the pivot row straight from S and
+//    scales the elements it needs.  The row scales are applied when the
+//    inverse is unscrambled.
+//  * The multipliers of step k (column k before the step) come from a copy
+//    that warp 0 wrote during step k-1, when it computed that column, so the
+//    owners of column k may overwrite it during step k.
+//  * Warp 0 computes the new column k+1, its pivot (over the rows not yet
+//    used) and the reciprocal; warps 1..7 update every other column, each
+//    thread one column and a stride of rows.  Rows are stored with an odd
+//    stride (ld = no | 1 double2), so a warp reading a column hits distinct
+//    banks.  det = product of the pivots times the permutation's sign.
 // At most 64 rows (no <= 64, checked by the caller).
 __device__ __forceinline__ void gj_body(int W, int no0, int no1, double* sbuf, long long sstride,
                                         int bstride, double* wscal, int w, int sct) {
@@ -399,16 +407,15 @@ __device__ __forceinline__ void gj_body(int W, int no0, int no1, double* sbuf, l
   const int no = sct ? no1 : no0;
   const int ld = no | 1;
   const int nn = no * no;
-  double2* const buf0 = gsm;
-  double2* const buf1 = gsm + bstride;
-  double2* const prow = gsm + 2 * bstride;  // [2][64]: scaled pivot row of the step, by parity
-  __shared__ double2 ipks[2];
+  double2* const A = gsm;
+  double2* const pcol = gsm + bstride;  // [2][64]: multipliers of the step, by parity
+  __shared__ double2 ipks[64];          // 1 / pivot of each step (the lazy row scales)
   __shared__ int piv[64];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   double2* g = reinterpret_cast<double2*>(sbuf) + ((long long)sct * W + w) * sstride;
   for (int e = tid; e < nn; e += kGreenThreads) {
     const int i = e / no;
-    buf0[i * ld + (e - i * no)] = g[e];
+    A[i * ld + (e - i * no)] = g[e];
   }
   __syncthreads();
 
@@ -416,19 +423,25 @@ __device__ __forceinline__ void gj_body(int W, int no0, int no1, double* sbuf, l
   const bool in0 = lane < no, in1 = lane + 32 < no;
   bool used0 = false, used1 = false;  // warp 0: rows lane, lane + 32 already pivots
   double2 det = make_double2(1.0, 0.0);
-  if (warp == 0) {  // pivot of column 0 and its scaled row
-    const double2 v0 = in0 ? buf0[lane * ld] : zero, v1 = in1 ? buf0[(lane + 32) * ld] : zero;
-    const int r = gj_pivot(v0, v1, in0, in1, lane);
-    const double2 p = buf0[r * ld];
+  // warp 0: the pivot of column 0 and its value, from the column in registers
+  auto pivot = [&](double2 v0, double2 v1, int col) {
+    const int rn = gj_pivot(v0, v1, in0 && !used0, in1 && !used1, lane);
+    const double2 sel = rn < 32 ? v0 : v1;
+    const double2 p = make_double2(__shfl_sync(0xffffffffu, sel.x, rn & 31),
+                                   __shfl_sync(0xffffffffu, sel.y, rn & 31));
     const double inv = 1.0 / (p.x * p.x + p.y * p.y);
-    const double2 ipk = make_double2(p.x * inv, -p.y * inv);
-    if (lane == (r & 31)) (r < 32 ? used0 : used1) = true;
-    for (int j = lane; j < no; j += 32) prow[j] = (j == 0) ? ipk : cmul(buf0[r * ld + j], ipk);
+    if (lane == (rn & 31)) (rn < 32 ? used0 : used1) = true;
     if (lane == 0) {
-      piv[0] = r;
-      ipks[0] = ipk;
-      det = p;
+      piv[col] = rn;
+      ipks[col] = make_double2(p.x * inv, -p.y * inv);
+      det = cmul(det, p);
     }
+  };
+  if (warp == 0) {
+    const double2 v0 = in0 ? A[lane * ld] : zero, v1 = in1 ? A[(lane + 32) * ld] : zero;
+    if (in0) pcol[lane] = v0;
+    if (in1) pcol[lane + 32] = v1;
+    pivot(v0, v1, 0);
   }
   __syncthreads();
 
@@ -442,74 +455,55 @@ __device__ __forceinline__ void gj_body(int W, int no0, int no1, double* sbuf, l
   const bool upd = warp > 0 && g0 < G;
   for (int k = 0; k < no; ++k) {
     const int cur = k & 1;
-    const double2* src = cur ? buf1 : buf0;
-    double2* dst = cur ? buf0 : buf1;
-    const double2* pr = prow + cur * 64;
+    const double2* pc = pcol + cur * 64;
     const int r = piv[k];
-    const double2 ipk = ipks[cur];
+    const double2 ipk = ipks[k];
     const int c = k + 1;
     if (warp == 0) {
       if (c < no) {
-        // new column c, then the next pivot among the unused rows
+        // the new column c (row r keeps its unscaled values), the next step's
+        // multipliers, then the pivot among the unused rows
+        const double2 prc = cmul(A[r * ld + c], ipk);
         double2 v0 = zero, v1 = zero;
-        const double2 prc = pr[c];
         if (in0) {
           const int i = lane;
-          v0 = (i == r) ? prc : csub(src[i * ld + c], cmul(src[i * ld + k], prc));
-          dst[i * ld + c] = v0;
+          v0 = A[i * ld + c];
+          if (i != r) {
+            v0 = csub(v0, cmul(pc[i], prc));
+            A[i * ld + c] = v0;
+          }
+          pcol[(cur ^ 1) * 64 + i] = v0;
         }
         if (in1) {
           const int i = lane + 32;
-          v1 = (i == r) ? prc : csub(src[i * ld + c], cmul(src[i * ld + k], prc));
-          dst[i * ld + c] = v1;
-        }
-        const int rn = gj_pivot(v0, v1, in0 && !used0, in1 && !used1, lane);
-        __syncwarp();
-        const double2 p = dst[rn * ld + c];
-        const double inv = 1.0 / (p.x * p.x + p.y * p.y);
-        const double2 ipn = make_double2(p.x * inv, -p.y * inv);
-        if (lane == (rn & 31)) (rn < 32 ? used0 : used1) = true;
-        // the new pivot row after this step, scaled by 1/p
-        const double2 f = src[rn * ld + k];
-        double2* pn = prow + (cur ^ 1) * 64;
-        for (int j = lane; j < no; j += 32) {
-          double2 v;
-          if (j == c) {
-            v = ipn;
-          } else if (j == k) {
-            const double2 t0 = cmul(f, ipk);
-            v = cmul(make_double2(-t0.x, -t0.y), ipn);
-          } else {
-            v = cmul(csub(src[rn * ld + j], cmul(f, pr[j])), ipn);
+          v1 = A[i * ld + c];
+          if (i != r) {
+            v1 = csub(v1, cmul(pc[i], prc));
+            A[i * ld + c] = v1;
           }
-          pn[j] = v;
+          pcol[(cur ^ 1) * 64 + i] = v1;
         }
-        if (lane == 0) {
-          piv[c] = rn;
-          ipks[cur ^ 1] = ipn;
-          det = cmul(det, p);
-        }
+        pivot(v0, v1, c);
       }
     } else if (upd && jc != c) {
       const int j = jc;
-      if (j == k) {  // the pivot column: -f / p, and 1 / p in the pivot row
+      if (j == k) {  // the pivot column: -(multiplier) / p, and 1 in the (lazy) pivot row
         for (int i = g0; i < no; i += G) {
-          const double2 t0 = cmul(src[i * ld + k], ipk);
-          dst[i * ld + j] = (i == r) ? ipk : make_double2(-t0.x, -t0.y);
+          const double2 t0 = cmul(pc[i], ipk);
+          A[i * ld + j] = (i == r) ? make_double2(1.0, 0.0) : make_double2(-t0.x, -t0.y);
         }
       } else {
-        const double2 prj = pr[j];
+        const double2 prj = cmul(A[r * ld + j], ipk);
         for (int i = g0; i < no; i += G)
-          dst[i * ld + j] = (i == r) ? prj : csub(src[i * ld + j], cmul(src[i * ld + k], prj));
+          if (i != r) A[i * ld + j] = csub(A[i * ld + j], cmul(pc[i], prj));
       }
     }
     __syncthreads();
   }
-  // unscramble: S^-1[i][r_k] = X[r_i][k]
-  const double2* X = (no & 1) ? buf1 : buf0;
+  // unscramble with the row scales: S^-1[i][r_k] = X[r_i][k] = A[r_i][k] / p_i
   for (int e = tid; e < nn; e += kGreenThreads) {
     const int i = e / no, k = e - (e / no) * no;
-    g[i * no + piv[k]] = X[piv[i] * ld + k];
+    g[i * no + piv[k]] = cmul(A[piv[i] * ld + k], ipks[i]);
   }
   if (tid == 0) {
     // sign of the permutation k -> r_k: (-1)^(no - cycles)
@@ -585,8 +579,8 @@ size_t green_smem_bytes(int nomax) {
          2 * size_t(kRowChunk) * nomax * sizeof(double) + size_t(kRowChunk) * (nomax + 1) * sizeof(double2);
 }
 
-// two row-padded copies of S (row stride nomax | 1) and two scaled pivot rows
-size_t gj_smem_bytes(int nomax) { return (2 * size_t(nomax) * (nomax | 1) + 128) * sizeof(double2); }
+// S with row stride nomax | 1 and two columns of multipliers
+size_t gj_smem_bytes(int nomax) { return (size_t(nomax) * (nomax | 1) + 128) * sizeof(double2); }
 
 cudaError_t launch_green_grouped(const GreenArgs* args, const BlockMap& m, int mode, size_t smem,
                                  cudaStream_t st) {

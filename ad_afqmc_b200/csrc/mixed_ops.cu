@@ -135,17 +135,18 @@ struct FbEpiU {
   template <int BN>
   __device__ void tile(int z, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t*) const {
-    const int g = mti * s.a_step + row;
+    const int g = mti * s.a_step + row, M = s.M, Nn = s.N;  // fields in registers before the stores
+    const long long l = ld;
     double* dst = part + (long long)z * zstride + g;
 #pragma unroll 1
     for (int ch = 0; ch < BN / 16; ++ch) {
       float v[16];
       src.load16(ch * 16, v);
-      if (g >= s.M) continue;
+      if (g >= M) continue;
       const int n0 = nti * s.b_step + ch * 16;
 #pragma unroll
       for (int i = 0; i < 16; ++i)
-        if (n0 + i < s.N) dst[(long long)(n0 + i) * ld] = (double)v[i];
+        if (n0 + i < Nn) dst[(long long)(n0 + i) * l] = (double)v[i];
     }
   }
 };
@@ -157,20 +158,32 @@ struct VhsEpiU {
   template <int BN>
   __device__ void tile(int, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t*) const {
+    // fields in registers before the bf16 stores
+    const int n_ = N, np = npc, M = s.M, Nn = s.N;
+    const long long l = ld, ws = wstride;
     const int q = mti * s.a_step + row;  // q = p*N + r
-    const int p = q / N, r = q - (q / N) * N;
+    const int p = q / n_, r = q - (q / n_) * n_;
+    bf16* const v0 = vp[0] + (long long)p * l + r;
+    bf16* const v1 = vp[1] + (long long)p * l + r;
+    bf16* const v2 = np > 2 ? vp[2] + (long long)p * l + r : nullptr;
 #pragma unroll 1
     for (int ch = 0; ch < BN / 16; ++ch) {
       float v[16];
       src.load16(ch * 16, v);
-      if (q >= s.M) continue;
+      if (q >= M) continue;
       const int n0 = nti * s.b_step + ch * 16;
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int n = n0 + i;
-        if (n < s.N) {
-          const int w = n >> 1, c = n & 1;
-          put_pieces_f(v[i], npc, vp, (long long)w * wstride + (long long)p * ld + c * N + r);
+        if (n < Nn) {
+          const long long off = (long long)(n >> 1) * ws + (n & 1) * n_;
+          const float x = v[i];
+          const bf16 h = __float2bfloat16_rn(x);
+          v0[off] = h;
+          const float rr = x - __bfloat162float(h);
+          const bf16 lo = __float2bfloat16_rn(rr);
+          v1[off] = lo;
+          if (np > 2) v2[off] = __float2bfloat16_rn(rr - __bfloat162float(lo));
         }
       }
     }
@@ -197,10 +210,28 @@ struct PropEpiU {
   template <int BN>
   __device__ void tile(int b, int mti, int, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t*) const {
+    // every field in a register first: the stores below go through float and
+    // bf16 pointers that the compiler cannot prove leave this struct alone
+    const int md = mode, np = npc, n_ = N, ncol = nc;
+    const float sc = scale;
+    const long long ld = bt_ld;
     const int p = mti * s.a_step + row;
-    const bool ok = p < N;
-    float* acol = acc + (long long)b * acc_bs + p;  // element (n, p) at acol[n * N]
-    const long long bbase = (long long)b * bt_bs;
+    const bool ok = p < n_;
+    float* const acol = acc + (long long)b * acc_bs + p;  // element (n, p) at acol[n * N]
+    const long long bb = (long long)b * bt_bs + p;
+    bf16* const q0 = bt[0] + bb;
+    bf16* const q1 = bt[1] + bb;
+    bf16* const q2 = np > 2 ? bt[2] + bb : nullptr;
+    double* const wo = md == PM_OUT ? wout + (long long)b * n_ * ncol + (long long)p * ncol : nullptr;
+    // split-BF16 pieces of x at offset `off` of this row's operand column
+    auto put = [&](float x, long long off) {
+      const bf16 h = __float2bfloat16_rn(x);
+      q0[off] = h;
+      const float r = x - __bfloat162float(h);
+      const bf16 l = __float2bfloat16_rn(r);
+      q1[off] = l;
+      if (np > 2) q2[off] = __float2bfloat16_rn(r - __bfloat162float(l));
+    };
 #pragma unroll 1
     for (int ch = 0; ch < BN / 16; ++ch) {
       float v[16];
@@ -210,42 +241,42 @@ struct PropEpiU {
       // all accumulator loads of the chunk first (independent, in flight together)
       float av[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) av[i] = (n0 + i < nc) ? acol[(long long)(n0 + i) * N] : 0.f;
+      for (int i = 0; i < 16; ++i) av[i] = (n0 + i < ncol) ? acol[(long long)(n0 + i) * n_] : 0.f;
 #pragma unroll
       for (int i = 0; i < 16; i += 2) {
         const int n = n0 + i;  // (re, im) pair of orbital j = n/2
-        if (n >= nc) break;
-        float* a0 = acol + (long long)n * N;
-        float* a1 = acol + (long long)(n + 1) * N;
+        if (n >= ncol) break;
+        float* a0 = acol + (long long)n * n_;
+        float* a1 = a0 + n_;
         float tr = v[i], ti = v[i + 1];
-        if (mode == PM_OUT) {
-          double* o = wout + (long long)b * N * nc + (long long)p * nc + n;
-          o[0] = (double)(av[i] + tr);
-          o[1] = (double)(av[i + 1] + ti);
+        if (md == PM_OUT) {
+          wo[n] = (double)(av[i] + tr);
+          wo[n + 1] = (double)(av[i + 1] + ti);
           continue;
         }
-        if (mode == PM_Y) {
+        if (md == PM_Y) {
           tr += av[i];
           ti += av[i + 1];
           *a0 = tr;
           *a1 = ti;
         } else {
-          tr *= scale;
-          ti *= scale;
+          tr *= sc;
+          ti *= sc;
           const float sr = av[i] + tr, si = av[i + 1] + ti;
           *a0 = sr;
           *a1 = si;
-          if (mode == PM_TLAST) {  // hand the finished sum to the closing half-step
+          if (md == PM_TLAST) {  // hand the finished sum to the closing half-step
             tr = sr;
             ti = si;
           }
         }
         // rows n (re) and n+1 (im) of the next B operand; columns [0,N): x, [N,2N): i*x
-        put_pieces_f(tr, npc, bt, bbase + (long long)n * bt_ld + p);
-        put_pieces_f(ti, npc, bt, bbase + (long long)(n + 1) * bt_ld + p);
-        if (mode != PM_TLAST) {
-          put_pieces_f(-ti, npc, bt, bbase + (long long)n * bt_ld + N + p);
-          put_pieces_f(tr, npc, bt, bbase + (long long)(n + 1) * bt_ld + N + p);
+        const long long o0 = (long long)n * ld, o1 = o0 + ld;
+        put(tr, o0);
+        put(ti, o1);
+        if (md != PM_TLAST) {
+          put(-ti, o0 + n_);
+          put(tr, o1 + n_);
         }
       }
     }

@@ -153,15 +153,46 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 16 columns of this thread's TMEM lane, load issued without waiting
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
+// wait for the issued TMEM loads; the destination registers pass through the
+// wait so that no use of them is scheduled before it
+__device__ __forceinline__ void tmem_wait_ld16x2(uint32_t (&r)[16], uint32_t (&q)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(q[0]), "+r"(q[1]),
+                 "+r"(q[2]), "+r"(q[3]), "+r"(q[4]), "+r"(q[5]), "+r"(q[6]), "+r"(q[7]),
+                 "+r"(q[8]), "+r"(q[9]), "+r"(q[10]), "+r"(q[11]), "+r"(q[12]), "+r"(q[13]),
+                 "+r"(q[14]), "+r"(q[15])
+               :
+               : "memory");
+}
+
 // 16 columns of the accumulator, summing the second accumulator group (if
-// any, BN columns further on) in FP32 round-to-nearest
+// any, BN columns further on) in FP32 round-to-nearest; both groups' loads
+// are in flight together
 __device__ __forceinline__ void acc_ld16(uint32_t taddr, int ngroups, int bn, float (&v)[16]) {
-  tmem_ld16(taddr, v);
-  if (ngroups == 2) {
-    float w[16];
-    tmem_ld16(taddr + bn, w);
+  uint32_t r[16], q[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] += w[i];
+  for (int i = 0; i < 16; ++i) q[i] = 0u;
+  tmem_ld16_issue(taddr, r);
+  if (ngroups == 2) tmem_ld16_issue(taddr + bn, q);
+  tmem_wait_ld16x2(r, q);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  if (ngroups == 2) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] += __uint_as_float(q[i]);
   }
 }
 
