@@ -193,11 +193,15 @@ struct VhsEpiU {
 // Modes of the propagator GEMMs.  The one-body factor is applied as
 // w + (e^{-dt h/2} - I) w: the tensor cores see only the small correction D
 // and the identity part is added exactly from the FP32 accumulator.
+// The Taylor series of e^{VHS} y runs in Horner form, z_T = y,
+// z_{n-1} = y + VHS z_n / n, down to z_0 = sum_{n <= T} VHS^n y / n!: every
+// term reads y from the FP32 accumulator and only the last one writes it back,
+// where the forward sum (acc += VHS^n y / n!) read and wrote it in each term.
 //   PM_Y     v = D w      : acc = w + v = y ; next B <- [y^T | (i y)^T]
-//   PM_T     v = VHS t    : t = v/n ; acc += t ; next B <- [t^T | (i t)^T]
-//   PM_TLAST v = VHS t    : t = v/n ; acc += t ; next B <- acc^T (finished sum)
+//   PM_H     v = VHS z_n  : z = acc + v/n   ; next B <- [z^T | (i z)^T]
+//   PM_HLAST v = VHS z_1  : z_0 = acc + v   ; acc = z_0 ; next B <- z_0^T
 //   PM_OUT   v = D acc    : walker = acc + v  (FP64 walker state)
-enum { PM_Y = 0, PM_T = 1, PM_TLAST = 2, PM_OUT = 3 };
+enum { PM_Y = 0, PM_H = 1, PM_HLAST = 2, PM_OUT = 3 };
 
 struct PropEpiU {
   int mode, npc, N, nc;
@@ -259,22 +263,19 @@ struct PropEpiU {
           ti += av[i + 1];
           *a0 = tr;
           *a1 = ti;
-        } else {
-          tr *= sc;
-          ti *= sc;
-          const float sr = av[i] + tr, si = av[i + 1] + ti;
-          *a0 = sr;
-          *a1 = si;
-          if (md == PM_TLAST) {  // hand the finished sum to the closing half-step
-            tr = sr;
-            ti = si;
+        } else {  // Horner step z = y + v / n, y in the accumulator
+          tr = av[i] + tr * sc;
+          ti = av[i + 1] + ti * sc;
+          if (md == PM_HLAST) {  // hand the finished sum to the closing half-step
+            *a0 = tr;
+            *a1 = ti;
           }
         }
         // rows n (re) and n+1 (im) of the next B operand; columns [0,N): x, [N,2N): i*x
         const long long o0 = (long long)n * ld, o1 = o0 + ld;
         put(tr, o0);
         put(ti, o1);
-        if (md != PM_TLAST) {
+        if (md != PM_HLAST) {
           put(-ti, o0 + n_);
           put(tr, o1 + n_);
         }
@@ -719,10 +720,11 @@ static int propagate_one(const Layout& L, const double* prep, double* work, doub
   if (rc != AFQ_OK) return rc;
   bf16** src = b1;
   bf16** dst = b0;
-  for (int n = 1; n < n_exp_terms; ++n) {
-    const int mode = (n == n_exp_terms - 1) ? PM_TLAST : PM_T;
+  // Horner: z_{n-1} = y + VHS z_n / n for n = T .. 1 (T = n_exp_terms - 1)
+  for (int n = n_exp_terms - 1; n >= 1; --n) {
+    const int mode = (n == 1) ? PM_HLAST : PM_H;
     rc = prop_launch<BN>(L, prep, work, s, nc, mode, 1.f / n, v, 2LL * N, L.Kv, vbs, 1, src, dst,
-                         nullptr, n, st);
+                         nullptr, n_exp_terms - n, st);
     if (rc != AFQ_OK) return rc;
     bf16** t = src;
     src = dst;

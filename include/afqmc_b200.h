@@ -60,7 +60,10 @@ enum { AFQ_SR_LOCAL = 0, AFQ_SR_GLOBAL = 1 };           /* sr z-formula */
 /* Problem sizes and method switches (fixed for one prepared buffer). */
 typedef struct afq_dims {
   int32_t norb;        /* N: orbitals                                        */
-  int32_t nocc[2];     /* electrons per spin (restricted walkers use nocc[0]) */
+  int32_t nocc[2];     /* electrons per spin (restricted walkers use nocc[0]), */
+                       /* 1..64 (AFQ_ERR_SHAPE above: the Green's-function   */
+                       /* and exchange kernels keep No x No blocks in shared  */
+                       /* memory; the reference has no such limit)            */
   int32_t nchol;       /* G: Cholesky vectors                                */
   int32_t nwalkers;    /* W                                                  */
   int32_t walker_type; /* AFQ_RESTRICTED / AFQ_UNRESTRICTED                  */
