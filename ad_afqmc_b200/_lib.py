@@ -85,11 +85,12 @@ class afq_tuning(C.Structure):
         ("prop_chunk", C.c_int32),
         ("qr_mode", C.c_int32),
         ("vhs_chunk", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("prop_bn", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
     KNOBS = ("fb_splitk", "fb_bn", "vhs_bn", "exch_bn", "f64_exch_bn", "max_stages", "grid_cap",
-             "prop_epi_groups", "prop_order", "prop_chunk", "qr_mode", "vhs_chunk")
+             "prop_epi_groups", "prop_order", "prop_chunk", "qr_mode", "vhs_chunk", "prop_bn")
 
     def as_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k in self.KNOBS}

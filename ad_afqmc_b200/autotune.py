@@ -32,6 +32,9 @@ Knobs (0 = the built-in rule):
                     chain per accumulator group (364 vs 276 us per launch at
                     N=200, G=1000, W=512).  Not searched: it changes results
                     beyond the last bits
+  prop_bn           column tile of the tensor-core propagator (several tiles
+                    per walker when narrower than 2 No; bit-identical results,
+                    slower at every measured shape, so not searched)
   grid_cap          CTAs of the persistent kernels (a batch-level knob: a
                     solve alone never gains from fewer CTAs, but overlapping
                     fragments can; ``tune_batch`` sweeps it for a whole batch)

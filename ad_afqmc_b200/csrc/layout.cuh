@@ -195,6 +195,9 @@ inline int make_layout(const afq_dims* d, Layout& L, const afq_tuning* record = 
   if (T.prop_chunk < 0 || T.prop_chunk > 2) return AFQ_ERR_ARG;
   if (T.qr_mode < 0 || T.qr_mode > 2) return AFQ_ERR_ARG;
   if (T.vhs_chunk < 0 || T.vhs_chunk > 2) return AFQ_ERR_ARG;
+  if (T.prop_bn != 0 && T.prop_bn != 16 && T.prop_bn != 32 && T.prop_bn != 48 && T.prop_bn != 64 &&
+      T.prop_bn != 80 && T.prop_bn != 96 && T.prop_bn != 128)
+    return AFQ_ERR_ARG;
   if (T.vhs_bn != 0 && T.vhs_bn != 64 && T.vhs_bn != 128) return AFQ_ERR_ARG;
   if (T.fb_splitk > 0) L.splitk = T.fb_splitk;
   for (int s = 0; s < 2; ++s) {

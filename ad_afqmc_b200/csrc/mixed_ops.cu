@@ -212,7 +212,7 @@ struct PropEpiU {
   long long bt_ld, bt_bs;
   double* wout;         // (W, N, nc) doubles
   template <int BN>
-  __device__ void tile(int b, int mti, int, int row, const AccSrc& src, const UmmaShape& s,
+  __device__ void tile(int b, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t*) const {
     // every field in a register first: the stores below go through float and
     // bf16 pointers that the compiler cannot prove leave this struct alone
@@ -240,8 +240,8 @@ struct PropEpiU {
     for (int ch = 0; ch < BN / 16; ++ch) {
       float v[16];
       src.load16(ch * 16, v);
-      if (!ok) continue;
-      const int n0 = ch * 16;
+      const int n0 = nti * BN + ch * 16;  // column tiles of BN when 2 No > BN
+      if (!ok || n0 >= ncol) continue;
       // all accumulator loads of the chunk first (independent, in flight together)
       float av[16];
 #pragma unroll
@@ -739,8 +739,23 @@ int mixed_propagate_walkers(const Layout& L, const double* prep, double* work,
                             double* const walkers[2], int n_exp_terms, cudaStream_t st) {
   for (int s = 0; s < L.np; ++s) {
     const int nc = 2 * L.no[s];
+    const int bn = L.tune.prop_bn;  // tuning: a narrower column tile (several per walker)
     int rc;
-    if (nc <= 16)
+    if (bn == 16)
+      rc = propagate_one<16>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (bn == 32)
+      rc = propagate_one<32>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (bn == 48)
+      rc = propagate_one<48>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (bn == 64)
+      rc = propagate_one<64>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (bn == 80)
+      rc = propagate_one<80>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (bn == 96)
+      rc = propagate_one<96>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (bn == 128)
+      rc = propagate_one<128>(L, prep, work, walkers[s], s, n_exp_terms, st);
+    else if (nc <= 16)
       rc = propagate_one<16>(L, prep, work, walkers[s], s, n_exp_terms, st);
     else if (nc <= 32)
       rc = propagate_one<32>(L, prep, work, walkers[s], s, n_exp_terms, st);

@@ -304,7 +304,11 @@ typedef struct afq_tuning {
                        /* chain per accumulator group), 1 the same, 2 chunks of four        */
                        /* 64-wide K blocks summed in FP32 round-to-nearest (less shared     */
                        /* memory left for the operand pipeline)                             */
-  int32_t reserved[4];
+  int32_t prop_bn;     /* column tile of the tensor-core propagator: 0 built-in (the        */
+                       /* narrowest of 16..128 that holds a walker's 2 No columns), or one  */
+                       /* of 16, 32, 48, 64, 80, 96, 128 (several tiles per walker when     */
+                       /* 2 No is wider)                                                    */
+  int32_t reserved[3];
 } afq_tuning;
 
 int afq_set_tuning(const afq_dims* d, const afq_tuning* t);

@@ -121,3 +121,28 @@ def test_step_under_accumulation_choices(rec, shape):
     finally:
         _lib.set_tuning(eng.dims, None)
     assert rel_err(got, o_pd["walkers"]) < 1e-4
+
+
+@pytest.mark.parametrize("bn", [16, 32, 48])
+def test_propagator_column_tiles_bit_identical(bn):
+    """prop_bn splits a walker's 2 No = 80 propagator columns over several
+    tensor-core tiles; every column's sum over K is the same chain in TMEM,
+    so a step is bit-identical to the built-in single tile."""
+    sys_ = make_system(200, (40, 40), 1000, seed=12, trial="rhf", chol_scale=0.25)
+    W = 6
+    walkers = near_trial_walkers(np.random.default_rng(4), sys_.mo_coeff, W, eps=0.1)
+    fields = np.random.default_rng(5).standard_normal((W, 1000))
+    d_trial, d_ham, d_wave, d_prop, _ = device_system(sys_, "restricted", 0.005, W, precision="mixed")
+    eng = d_prop.engine(d_ham, d_trial, d_wave)
+    out = []
+    try:
+        for rec in ({}, {"prop_bn": bn}):
+            _lib.set_tuning(eng.dims, _lib.afq_tuning.from_dict(rec) if rec else None)
+            eng.ensure_workspace()
+            pd = d_prop.init_prop_data(d_trial, d_wave, d_ham, 0, init_walkers=RHFWalkers(walkers.copy()))
+            pd = d_prop.propagate_constrained(d_trial, d_ham, pd, fields, d_wave)
+            out.append((pd["walkers"].data.clone(), pd["weights"].clone()))
+    finally:
+        _lib.set_tuning(eng.dims, None)
+    assert torch.equal(out[0][0], out[1][0])
+    assert torch.equal(out[0][1], out[1][1])
