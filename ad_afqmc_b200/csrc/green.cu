@@ -41,19 +41,20 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // Gauss-Jordan inverse with partial pivoting of the No x No complex S in
-// shared memory, in place, by the whole CTA (kGreenThreads threads); returns
-// det S in thread 0.
+// shared memory, in place, by the whole CTA (T threads); returns det S in
+// thread 0.
+template <int T>
 __device__ double2 gauss_jordan_cta(double2* S, double2* colk, int* perm, double2* ipk_s, int no) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  constexpr int T = kGreenThreads;
+  constexpr int Q = 4096 / T;  // elements of a 64 x 64 S per thread
   const int npairs = no * no;
   // Each elimination step: warp 0 alone finds the pivot (first max of
   // |re|+|im| in column k, as LAPACK izamax), swaps it into row k, keeps
   // column k and scales row k by 1/p (= conj(p)/|p|^2); then every thread
   // updates its fixed elements.  Two block barriers per step.
-  int my_i[16], my_j[16];
+  int my_i[Q], my_j[Q];
 #pragma unroll
-  for (int q = 0; q < 16; ++q) {
+  for (int q = 0; q < Q; ++q) {
     const int e = tid + q * T;
     my_i[q] = e < npairs ? e / no : -1;
     my_j[q] = e < npairs ? e - (e / no) * no : 0;
@@ -98,7 +99,7 @@ __device__ double2 gauss_jordan_cta(double2* S, double2* colk, int* perm, double
     __syncthreads();
     const double2 ipk = *ipk_s;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
+    for (int q = 0; q < Q; ++q) {
       const int i = my_i[q], j = my_j[q];
       if (i < 0 || i == k) continue;
       const double2 f = colk[i];
@@ -127,11 +128,15 @@ __device__ double2 gauss_jordan_cta(double2* S, double2* colk, int* perm, double
 
 // mode 0: the whole computation; 1: S = C^T W only, into a.sbuf; 2: Theta
 // and its outputs from S^-1 in a.sbuf (the inverse and det by gj_kernel).
+// T threads: 256, or 512 where the staging allows one CTA per SM only (each
+// warp then owns one column tile instead of up to two).
+template <int T>
 __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, int sct) {
   extern __shared__ double2 sm[];
   const GreenSector& S_ = a.sec[sct];
   const int N = a.N, no = S_.no, tid = threadIdx.x;
-  constexpr int T = kGreenThreads;
+  constexpr int NW = T / 32;                 // warps
+  constexpr int SL = (16 + NW - 1) / NW;     // column tiles per warp (2 No <= 128: 16 tiles)
 
   double2* S = sm;                          // no*no
   double2* colk = S + no * no;              // 64
@@ -177,9 +182,9 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
                        : nullptr;
   const int npairs = no * no;
   if (mode != 2) {
-  double sacc[2][8][2];
+  double sacc[SL][8][2];
 #pragma unroll
-  for (int sl = 0; sl < 2; ++sl)
+  for (int sl = 0; sl < SL; ++sl)
 #pragma unroll
     for (int mi = 0; mi < 8; ++mi) sacc[sl][mi][0] = sacc[sl][mi][1] = 0.0;
   load_chunk(0, true);
@@ -201,8 +206,8 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
         afr[mi] = (mi < mtiles && kin && m < no) ? mocc[kr * no + m] : 0.0;
       }
 #pragma unroll
-      for (int sl = 0; sl < 2; ++sl) {
-        const int ni = warp + sl * 8;
+      for (int sl = 0; sl < SL; ++sl) {
+        const int ni = warp + sl * NW;
         if (ni < ntiles) {  // warp-uniform
           const int n = ni * 8 + (lane >> 2);
           const double b = (kin && n < nc2) ? stageD[kr * sd + n] : 0.0;
@@ -215,8 +220,8 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
     __syncthreads();
   }
 #pragma unroll
-  for (int sl = 0; sl < 2; ++sl) {
-    const int ni = warp + sl * 8;
+  for (int sl = 0; sl < SL; ++sl) {
+    const int ni = warp + sl * NW;
     if (ni < ntiles) {
 #pragma unroll
       for (int mi = 0; mi < 8; ++mi) {
@@ -241,7 +246,7 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
 
   // ---- Gauss-Jordan inverse with partial pivoting, det ----------------------
   __shared__ double2 ipk_s;
-  const double2 det = gauss_jordan_cta(S, colk, perm, &ipk_s, no);
+  const double2 det = gauss_jordan_cta<T>(S, colk, perm, &ipk_s, no);
   if (tid == 0 && a.wscal) {
     a.wscal[(long long)w * 16 + 4 + 2 * sct] = det.x;
     a.wscal[(long long)w * 16 + 5 + 2 * sct] = det.y;
@@ -273,9 +278,9 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
     // R[2i+1][2j] = -Im s_ij, generated in the B fragments
     {
       const int rtiles = (rows + 7) >> 3;  // <= 4
-      double tacc[2][4][2];
+      double tacc[SL][4][2];
 #pragma unroll
-      for (int sl = 0; sl < 2; ++sl)
+      for (int sl = 0; sl < SL; ++sl)
 #pragma unroll
         for (int ri = 0; ri < 4; ++ri) tacc[sl][ri][0] = tacc[sl][ri][1] = 0.0;
       for (int kk = 0; kk < nc2; kk += 4) {
@@ -288,8 +293,8 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
           afr[ri] = (ri < rtiles && kin && r < rows) ? stageD[r * sd + k] : 0.0;
         }
 #pragma unroll
-        for (int sl = 0; sl < 2; ++sl) {
-          const int ni = warp + sl * 8;
+        for (int sl = 0; sl < SL; ++sl) {
+          const int ni = warp + sl * NW;
           if (ni < ntiles) {  // warp-uniform
             const int n = ni * 8 + (lane >> 2);
             double b = 0.0;
@@ -304,8 +309,8 @@ __device__ __forceinline__ void green_body(const GreenArgs& a, int mode, int w, 
         }
       }
 #pragma unroll
-      for (int sl = 0; sl < 2; ++sl) {
-        const int ni = warp + sl * 8;
+      for (int sl = 0; sl < SL; ++sl) {
+        const int ni = warp + sl * NW;
         if (ni >= ntiles) continue;
 #pragma unroll
         for (int ri = 0; ri < 4; ++ri) {
@@ -522,15 +527,16 @@ __device__ __forceinline__ void gj_body(int W, int no0, int no1, double* sbuf, l
   }
 }
 
-__global__ void __launch_bounds__(kGreenThreads) green_kernel(GreenArgs a, int mode) {
-  green_body(a, mode, blockIdx.x, blockIdx.y);
+template <int T>
+__global__ void __launch_bounds__(T) green_kernel(GreenArgs a, int mode) {
+  green_body<T>(a, mode, blockIdx.x, blockIdx.y);
 }
 
 __global__ void __launch_bounds__(kGreenThreads) green_kernel_grouped(const GreenArgs* A, BlockMap m,
                                                                       int mode) {
   int local;
   const GreenArgs& a = A[block_owner(m, blockIdx.x, local)];
-  green_body(a, mode, local % a.W, local / a.W);
+  green_body<kGreenThreads>(a, mode, local % a.W, local / a.W);
 }
 
 __global__ void __launch_bounds__(kGreenThreads, 4)
@@ -611,8 +617,11 @@ cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   int nomax = 0;
   for (int s = 0; s < a.ns; ++s) nomax = a.sec[s].no > nomax ? a.sec[s].no : nomax;
   const size_t smem = green_smem_bytes(nomax);
-  cudaError_t e = cudaFuncSetAttribute(green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  // staging above ~113 KB leaves one CTA per SM: 16 warps instead of 8 then
+  const bool wide = smem > 113 * 1024;
+  auto kernel = wide ? green_kernel<2 * kGreenThreads> : green_kernel<kGreenThreads>;
+  const int threads = wide ? 2 * kGreenThreads : kGreenThreads;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid(a.W, a.ns);
   ProfScope ps(K_GREEN, st);
@@ -620,11 +629,11 @@ cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   for (int s = 0; s < a.ns; ++s)
     need_theta = need_theta || a.sec[s].theta || a.sec[s].gout || a.sec[s].rh1 || a.sec[s].gtb[0];
   if (!a.sbuf || !need_theta) {  // one kernel: S, its inverse and det, Theta and outputs
-    green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 0);
+    kernel<<<grid, threads, smem, st>>>(a, 0);
     return cudaGetLastError();
   }
   // S into a.sbuf; warp-level inverse and det; Theta and its outputs
-  green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 1);
+  kernel<<<grid, threads, smem, st>>>(a, 1);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const int bstride = nomax * (nomax | 1);
   const size_t gsmem = gj_smem_bytes(nomax);
@@ -634,7 +643,7 @@ cudaError_t launch_green(const GreenArgs& a, cudaStream_t st) {
   gj_kernel<<<grid, kGreenThreads, gsmem, st>>>(a.W, a.sec[0].no, a.ns > 1 ? a.sec[1].no : 0,
                                                 a.sbuf, a.sstride, bstride, a.wscal);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  green_kernel<<<grid, kGreenThreads, smem, st>>>(a, 2);
+  kernel<<<grid, threads, smem, st>>>(a, 2);
   return cudaGetLastError();
 }
 
