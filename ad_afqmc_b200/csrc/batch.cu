@@ -141,6 +141,7 @@ int afq_batch_create(int32_t n, const afq_dims* dims, const void* const* prepare
     p.ldxb = l.Gb;
     p.field_step = (long long)l.W * l.G;
     p.fbpart = Wk[f] + l.w_fbpart;
+    p.f32 = 1;  // batches are mixed precision: FP32 partials
     p.alpha = (double)l.mult;
     p.sdt = sqrt(dims[f].dt);
     p.fields = fields[f];

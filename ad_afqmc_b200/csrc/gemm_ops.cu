@@ -60,8 +60,10 @@ __global__ void __launch_bounds__(Cfg::NT) fb_gemm_kernel(F64Operand A, F64Opera
 // field preparation (one CTA per walker)
 // ---------------------------------------------------------------------------
 // one compiled copy for the solo and the grouped kernel (identical rounding)
+// fbpart: split-K partial sums of the force bias, FP64 (FP64 path) or FP32
+// (f32: the tensor-core path's FP32 accumulators, stored as they are)
 __device__ __noinline__ void prep_body(int W, int G, long long Gpad, int splitk,
-                                          const double* fbpart, double alpha, const double* fields,
+                                          const void* fbpart, int f32, double alpha, const double* fields,
                                           const double* mf, double sdt, double* xt, double* wscal,
                                           double* fb_out, int npc, bf16* xb0, bf16* xb1, bf16* xb2,
                                           long long ldxb, int w) {
@@ -72,9 +74,18 @@ __device__ __noinline__ void prep_body(int W, int G, long long Gpad, int splitk,
   double sr = 0, si = 0, br = 0, bi = 0;
   for (int g = tid; g < G; g += blockDim.x) {
     double fr = 0.0, fi = 0.0;
-    for (int z = 0; z < splitk; ++z) {
-      fr += fbpart[z * zs + (2LL * w) * Gpad + g];
-      fi += fbpart[z * zs + (2LL * w + 1) * Gpad + g];
+    if (f32) {
+      const float* fp = static_cast<const float*>(fbpart);
+      for (int z = 0; z < splitk; ++z) {
+        fr += (double)fp[z * zs + (2LL * w) * Gpad + g];
+        fi += (double)fp[z * zs + (2LL * w + 1) * Gpad + g];
+      }
+    } else {
+      const double* dp = static_cast<const double*>(fbpart);
+      for (int z = 0; z < splitk; ++z) {
+        fr += dp[z * zs + (2LL * w) * Gpad + g];
+        fi += dp[z * zs + (2LL * w + 1) * Gpad + g];
+      }
     }
     fr *= alpha;
     fi *= alpha;
@@ -119,19 +130,19 @@ __device__ __noinline__ void prep_body(int W, int G, long long Gpad, int splitk,
 }
 
 __global__ void __launch_bounds__(256) prep_kernel(int W, int G, long long Gpad, int splitk,
-                                                   const double* fbpart, double alpha,
+                                                   const void* fbpart, int f32, double alpha,
                                                    const double* fields, const double* mf,
                                                    double sdt, double* xt, double* wscal,
                                                    double* fb_out, int npc, bf16* xb0, bf16* xb1,
                                                    bf16* xb2, long long ldxb) {
-  prep_body(W, G, Gpad, splitk, fbpart, alpha, fields, mf, sdt, xt, wscal, fb_out, npc, xb0, xb1,
-            xb2, ldxb, blockIdx.x);
+  prep_body(W, G, Gpad, splitk, fbpart, f32, alpha, fields, mf, sdt, xt, wscal, fb_out, npc, xb0,
+            xb1, xb2, ldxb, blockIdx.x);
 }
 
 __global__ void __launch_bounds__(256) prep_kernel_grouped(const PrepArgs* A, BlockMap m, int step) {
   int local;
   const PrepArgs& a = A[block_owner(m, blockIdx.x, local)];
-  prep_body(a.W, a.G, a.Gpad, a.splitk, a.fbpart, a.alpha, a.fields + (long long)step * a.field_step,
+  prep_body(a.W, a.G, a.Gpad, a.splitk, a.fbpart, a.f32, a.alpha, a.fields + (long long)step * a.field_step,
             a.mf, a.sdt, a.xt, a.wscal, nullptr, a.npc, a.xb[0], a.xb[1], a.xb[2], a.ldxb, local);
 }
 
@@ -486,7 +497,7 @@ cudaError_t launch_prep(const Layout& L, const double* prep, double* work, const
   ProfScope ps(K_PREP, st);
   bf16* xb[3] = {nullptr, nullptr, nullptr};
   if (L.mixed) piece_ptrs(work, L.v_xt, L.v_xt_ps, L.npc, xb);
-  prep_kernel<<<L.W, 256, 0, st>>>(L.W, L.G, L.Gpad, L.splitk, work + L.w_fbpart,
+  prep_kernel<<<L.W, 256, 0, st>>>(L.W, L.G, L.Gpad, L.splitk, work + L.w_fbpart, L.mixed ? 1 : 0,
                                    (double)L.mult, fields, prep + L.p_mf, sqrt(dt),
                                    work + L.w_xt, work + L.w_wscal, fb_out, L.npc, xb[0], xb[1],
                                    xb[2], L.Gb);

@@ -128,16 +128,17 @@ __global__ void walker_t_grouped(const WalkerTArgs* A, BlockMap m) {
 // epilogues
 // ---------------------------------------------------------------------------
 // C^T: rows g (Cholesky vector) = TMEM lanes, columns (w, re/im); the partial
-// sums land in part[z][(w,c)][g] so that a warp's stores are contiguous in g
+// sums land in part[z][(w,c)][g] so that a warp's stores are contiguous in g,
+// as the FP32 values the accumulator holds (the prep kernel sums them in FP64)
 struct FbEpiU {
-  double* part;
+  float* part;
   long long ld, zstride;
   template <int BN>
   __device__ void tile(int z, int mti, int nti, int row, const AccSrc& src, const UmmaShape& s,
                        uint8_t*) const {
     const int g = mti * s.a_step + row, M = s.M, Nn = s.N;  // fields in registers before the stores
     const long long l = ld;
-    double* dst = part + (long long)z * zstride + g;
+    float* dst = part + (long long)z * zstride + g;
 #pragma unroll 1
     for (int ch = 0; ch < BN / 16; ++ch) {
       float v[16];
@@ -146,7 +147,7 @@ struct FbEpiU {
       const int n0 = nti * s.b_step + ch * 16;
 #pragma unroll
       for (int i = 0; i < 16; ++i)
-        if (n0 + i < Nn) dst[(long long)(n0 + i) * l] = (double)v[i];
+        if (n0 + i < Nn) dst[(long long)(n0 + i) * l] = v[i];
     }
   }
 };
@@ -640,11 +641,12 @@ int fb_launch(const Layout& L, const double* prep, double* work, cudaStream_t st
   const int ks = (int)((kblocks + per - 1) / per);
   P.s.ksplit = ks;
   P.s.kchunk = (int)(per * kUBK);
+  float* part = reinterpret_cast<float*>(work + L.w_fbpart);
   for (int z = ks; z < L.splitk; ++z)
-    if (cudaMemsetAsync(work + L.w_fbpart + z * 2LL * L.W * L.Gpad, 0,
-                        sizeof(double) * 2LL * L.W * L.Gpad, st) != cudaSuccess)
+    if (cudaMemsetAsync(part + z * 2LL * L.W * L.Gpad, 0, sizeof(float) * 2LL * L.W * L.Gpad, st) !=
+        cudaSuccess)
       return AFQ_ERR_CUDA;  // (while recording a batch: once, on the legacy stream, at build time)
-  P.epi.part = work + L.w_fbpart;
+  P.epi.part = part;
   P.epi.ld = L.Gpad;
   P.epi.zstride = 2LL * L.W * L.Gpad;
   P.s.ngroups = 2;

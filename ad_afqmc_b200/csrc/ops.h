@@ -165,7 +165,8 @@ struct GjArgs {
 struct PrepArgs {
   int W, G, splitk, npc;
   long long Gpad, ldxb, field_step;  // doubles between the fields of consecutive steps
-  const double* fbpart;
+  const void* fbpart;                // FP32 partials (tensor-core force bias)
+  int f32;
   double alpha, sdt;
   const double* fields;              // fields of step 0
   const double* mf;
