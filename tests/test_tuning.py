@@ -41,7 +41,10 @@ def test_record_changes_choice_and_workspace_follows():
 
 @pytest.mark.parametrize("rec", [{"fb_splitk": 9}, {"fb_bn": 96}, {"vhs_bn": 256}, {"max_stages": 1},
                                  {"exch_bn": 64},       # 2 No = 80 columns do not fit 64
-                                 {"f64_exch_bn": 100}, {"grid_cap": -1}])
+                                 {"f64_exch_bn": 100}, {"grid_cap": -1},
+                                 {"prop_chunk": 3}, {"vhs_chunk": 3}, {"qr_mode": 3},
+                                 {"prop_bn": 40},       # not a compiled column tile
+                                 {"prop_bn": -16}, {"prop_order": 2}, {"prop_epi_groups": 4}])
 def test_invalid_records_rejected_and_not_registered(rec):
     d = _dims()
     before = _lib.get_tuning(d).as_dict()
@@ -78,3 +81,20 @@ def test_autotuner_cache_roundtrip(tmp_path):
     tu.save()
     assert json.loads(path.read_text())[key]["tuning"] == {"fb_splitk": 4}
     assert Autotuner(cache_path=str(path)).cache == tu.cache
+
+
+def test_accumulation_and_tile_knobs_accepted():
+    """The knobs that change how the mixed GEMMs accumulate K (prop_chunk,
+    vhs_chunk: 2 = FP32 chunk sums), the propagator's column tile and the QR
+    placement are registered and read back; 0 keeps the built-in choice."""
+    d = _dims(W=64)
+    try:
+        rec = {"prop_chunk": 2, "vhs_chunk": 2, "prop_bn": 48, "qr_mode": 2}
+        _lib.set_tuning(d, _lib.afq_tuning.from_dict(rec))
+        t = _lib.get_tuning(d).as_dict()
+        for k, v in rec.items():
+            assert t[k] == v
+    finally:
+        _lib.set_tuning(d, None)
+    t = _lib.get_tuning(d).as_dict()
+    assert t["prop_chunk"] == 0 and t["vhs_chunk"] == 0 and t["prop_bn"] == 0 and t["qr_mode"] == 0
