@@ -319,9 +319,10 @@ def measure_config(name, precision, steps, warmup, nb_acc):
     return out
 
 # DRAM bytes (read + written) per propagator launch, mean over the 7 launches
-# of one step, from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
-# bench workload (N=200, No=40, G=1000, 512 walkers, mixed).
-PROP_DRAM_BYTES_PER_LAUNCH = 257510875
+# of one step, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, caches
+# flushed before each launch) on the bench workload (N=200, No=40, G=1000,
+# 512 walkers, mixed, Taylor terms in Horner form).
+PROP_DRAM_BYTES_PER_LAUNCH = 243791506
 
 
 def main():
@@ -589,8 +590,9 @@ def main():
     else:
         # the propagator GEMMs (7 launches per step, the largest share of a block), HBM-bound:
         # algorithmic bytes of one step per spin sector s (nc = 2 No_s, npc bf16 pieces):
-        #   5 Taylor terms: VHS pieces W N 2N, iterate pieces W nc 2N, FP32 accumulator read and
-        #     written (W nc N), next iterate pieces W nc 2N (the last term: N columns)
+        #   5 Taylor terms in Horner form: VHS pieces W N 2N, iterate pieces W nc 2N, FP32 y read
+        #     from the accumulator (W nc N); next iterate pieces W nc 2N, except the last term,
+        #     which writes the finished sum to the accumulator and its pieces (N columns)
         #   2 one-body half-steps: (e^{-dt h/2} - I) pieces N N, walker/sum pieces W nc N,
         #     accumulator read (+ written by the first), next pieces W nc 2N / walker W N nc
         #     doubles out (the second)
@@ -600,8 +602,8 @@ def main():
         for s_ in range(nsec):
             nc = 2 * sys_.nelec[s_]
             bf = 2.0 * npc
-            taylor = (W * N * 2 * N * bf + W * nc * 2 * N * bf + 2 * W * nc * N * 4.0)
-            step_bytes += 5 * taylor + 4 * W * nc * 2 * N * bf + W * nc * N * bf
+            taylor = (W * N * 2 * N * bf + W * nc * 2 * N * bf + W * nc * N * 4.0)
+            step_bytes += 5 * taylor + 4 * W * nc * 2 * N * bf + W * nc * N * (bf + 4.0)
             step_bytes += 2 * (N * N * bf + W * nc * N * bf)           # the two half-steps' operands
             step_bytes += 2 * W * nc * N * 4.0 + W * nc * 2 * N * bf   # first half-step: acc r/w, pieces
             step_bytes += W * nc * N * 4.0 + W * N * nc * 8.0          # second: acc read, walker out
